@@ -1,0 +1,425 @@
+"""Benchmark of the McSART engine: SART iterations/s on one or more B200s.
+
+Workload (default): the motion-compensated McSART configuration, volume
+128x128x96 at 2 mm, flat detector 256x192 at 1.2 mm, SAD/SDD 1000/1500 mm,
+360 views over 360 degrees at 15 views/s with a 5DCT breathing model.  One
+step is one outer iteration = one image-update pass over all 360 views (warp,
+project, residual, backproject, normalise, inverse warp, update) plus one
+DVF-update pass over 359 views, i.e. host_AUMISART with op_iter = [1, 0].
+Inputs are seeded synthetic data of that shape (phantom, smooth random DVF,
+projections of the warped phantom), generated outside the timed region.
+
+  value   iterations/s through the device-resident driver, inputs in HBM,
+          L2 flushed (256 MiB write) before every timed step, device time by
+          CUDA events; whole job over N replicas (one per GPU, no data-path
+          collective: the path does not shard, see the design notes).
+  e2e     iterations/s through the host-pointer entry point mcsart_aumisart
+          (host_AUMISART's interface): H2D of the step's inputs from pinned
+          memory, the iteration, D2H of image, residuals, norms, alpha_x.
+  --impl reference   the reference's path on the host cores: the FP32 OpenMP
+          transcription of the reference kernels (the reference has no CPU
+          code of its own), on a bounded sample of views, extrapolated.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--config", default="c2")
+    ap.add_argument("--cpu-views", type=int, default=0,
+                    help="views per pass in the CPU sample (0 = auto)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the mixed-precision and fast-FP32 side measurements")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms in the background."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        under = [s for s in sm if mx and s > 0.5 * mx] or sm
+        return {"sm_mhz": float(np.median(under)) if under else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ----------------------------------------------------------------- problem
+def build_problem(ctx, torch, cfg_name: str, seed: int = 0):
+    """Seeded problem; projections made by the engine's own warp + projector."""
+    from mcsart_b200 import synthetic as S
+    p = S.make_problem(cfg_name, seed)
+    g = p.geo
+    dev = torch.device("cuda", torch.cuda.current_device())
+    truth = torch.as_tensor(p.truth, device=dev)
+    fields = [torch.as_tensor(f, device=dev) for f in p.fields] if p.fields else None
+    proj = torch.empty((p.cfg.n_views, g["nb"], g["na"]), dtype=torch.float32, device=dev)
+    tmp = torch.empty_like(truth)
+    for v in range(p.cfg.n_views):
+        src = truth
+        if fields is not None:
+            ctx.host_deform(tmp, truth, g["nx"], g["ny"], g["nz"],
+                            np.float32(p.volumes[v] - p.volumes[0]),
+                            np.float32(p.flows[v] - p.flows[0]), *fields)
+            src = tmp
+        ctx.host_projection(proj[v], src, float(p.angles[v]), g["SO"], g["SD"], g["da"], g["na"],
+                            g["ai"], g["db"], g["nb"], g["bi"], g["nx"], g["ny"], g["nz"])
+    ctx.synchronize()
+    return p, proj, fields
+
+
+def algorithmic_bytes(p) -> dict:
+    """Compulsory bytes per launch of the driver's kernels (FP32 storage)."""
+    g = p.geo
+    V = g["nx"] * g["ny"] * g["nz"]
+    P = g["na"] * g["nb"]
+    return {
+        # read the warped volume, the measured view; write residual + (residual, ones) pairs
+        "fp_image": 4 * V + 4 * P + 4 * P + 8 * P,
+        # read img, img0, ones; read the measured view; write the pairs
+        "fp_motion": 12 * V + 4 * P + 8 * P,
+        # read the pairs; write the ratio volume
+        "bp_div": 8 * P + 4 * V,
+        # read volume (+ its update), write volume and its y-fastest copy
+        "bp_div_add": 8 * P + 12 * V,
+        # read img, 6 fields; write warped volume and its y-fastest copy
+        "warp_fwd": 4 * V + 24 * V + 8 * V,
+        # read ratio, 6 fields, img; write img
+        "warp_back_add": 4 * V + 24 * V + 8 * V,
+        # read img, 6 fields; write img0, ones and their copies
+        "motion_prep": 4 * V + 24 * V + 16 * V,
+        # read ratio, img, read+write 6 fields
+        "field_update": 8 * V + 48 * V,
+    }
+
+
+def measured_peaks() -> dict:
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
+    except (OSError, KeyError, ValueError):
+        return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+# --------------------------------------------------------------- CPU side
+def cpu_sample(p, proj_host, views: int, threads: int):
+    """One image pass and one DVF-update pass of the FP32 OpenMP transcription
+    over `views` views each; returns (seconds, iterations/s extrapolated)."""
+    from oracle import oracle as O
+    O.set_num_threads(threads)
+    nv = p.cfg.n_views
+    views = max(2, min(views, nv))
+    it = dict(n_iter=2, op_iter=np.array([1, 0], np.int32), n_views=nv, outIter=1,
+              volumes=p.volumes, flows=p.flows, angles=p.angles, **{"lambda": p.cfg.lam})
+    t0 = time.perf_counter()
+    O.aumisart(p.img0, proj_host, p.geo, it, p.fields, prec="cpu", view_lo=0, view_hi=views)
+    dt = time.perf_counter() - t0
+    # image pass: `views` views; motion pass: views-1 views (starts at view 1)
+    per_view = dt / (2 * views - 1)
+    t_iter = per_view * (nv + (nv - 1))
+    return dt, 1.0 / t_iter, views
+
+
+def cpu_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def run_reference_arm(args, rank: int):
+    """--impl reference: the reference's path on the host cores (FP32 OpenMP port)."""
+    if rank != 0:
+        return
+    from mcsart_b200 import synthetic as S
+    p = S.make_problem(args.config, 0)
+    # measured projections from the oracle port of the reference projector (CPU)
+    from oracle import oracle as O
+    threads = cpu_threads()
+    O.set_num_threads(threads)
+    proj = np.zeros((p.cfg.n_views, p.cfg.nb, p.cfg.na), np.float32)
+    views = args.cpu_views or 6
+    # only the views the sample touches need measured data
+    for v in range(views + 1):
+        vol = O.deform(p.truth, np.float32(p.volumes[v] - p.volumes[0]),
+                       np.float32(p.flows[v] - p.flows[0]), p.fields, prec="cpu")
+        proj[v] = O.projection(vol, float(p.angles[v]), p.geo, prec="cpu")
+    for _ in range(args.warmup):
+        cpu_sample(p, proj, views, threads)
+    times, rates = [], []
+    for _ in range(args.steps):
+        dt, rate, _ = cpu_sample(p, proj, views, threads)
+        times.append(dt)
+        rates.append(rate)
+    value = float(np.median(rates))
+    sample = (f"{views} views of the image pass + {views - 1} of the DVF-update pass of "
+              f"{args.config} per step, extrapolated linearly to {p.cfg.n_views} + "
+              f"{p.cfg.n_views - 1} views")
+    line = {"impl": "reference", "metric": "McSART iterations/s", "value": value,
+            "unit": "iterations/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000.0 / value, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": config_dict(p, args),
+            "cpu_baseline": {"value": value, "unit": "iterations/s", "cores": threads,
+                             "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": "iterations/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+            "note": "the reference has no CPU implementation; this is the FP32 OpenMP "
+                    "transcription of its kernels and host_AUMISART loop"}
+    print(json.dumps(line), flush=True)
+
+
+def config_dict(p, args) -> dict:
+    c = p.cfg
+    return {"workload": f"{args.config}: {c.name}; one step = host_AUMISART with op_iter [1, 0]",
+            "volume": [c.nx, c.ny, c.nz], "voxel_mm": c.vox_mm, "detector": [c.na, c.nb],
+            "pitch_mm": c.pitch_mm, "views": c.n_views, "sad_sdd_mm": [1000, 1500],
+            "lambda": c.lam, "l2": "flushed before every timed step (256 MiB write)"}
+
+
+# -------------------------------------------------------------- GPU side
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference_arm(args, rank)
+        return
+
+    import torch
+    import torch.distributed as dist
+    import mcsart_b200 as m
+
+    torch.cuda.set_device(local)
+    dist_on = world > 1
+    if dist_on:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    ctx = m.Context(local, stream=stream)
+    p, proj, fields = build_problem(ctx, torch, args.config, seed=rank)
+    g = p.geo
+    nv = p.cfg.n_views
+    V = g["nx"] * g["ny"] * g["nz"]
+    op = np.array([1, 0], np.int32)
+    img = torch.zeros((g["nz"], g["ny"], g["nx"]), dtype=torch.float32, device="cuda")
+    F = torch.stack(fields).contiguous()
+    F0 = F.clone()
+    norm = torch.zeros(2 * nv, device="cuda")
+    resid = torch.zeros((nv, g["nb"], g["na"]), device="cuda")
+    flush = torch.empty(256 * 2**20 // 4, dtype=torch.float32, device="cuda")
+
+    def step(opts, img_t, F_t):
+        ctx.aumisart_device(geo=g, n_views=nv, lambda_=p.cfg.lam, angles=p.angles,
+                            volumes=p.volumes, flows=p.flows, img=img_t, proj=proj, fields=F_t,
+                            resid=resid, norm=norm, n_iter=2, op_iter=op, options=opts)
+
+    def timed(opts, steps, warmup, img_t, F_t, count_launches=False):
+        for _ in range(warmup):
+            step(opts, img_t, F_t)
+        torch.cuda.synchronize()
+        if dist_on:
+            dist.barrier()
+        torch.cuda.synchronize()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(steps)]
+        l0 = ctx.launches
+        for e0, e1 in ev:
+            flush.fill_(1.0)  # evict L2 between steps (not timed)
+            e0.record(stream)
+            step(opts, img_t, F_t)
+            e1.record(stream)
+        torch.cuda.synchronize()
+        launches = ctx.launches - l0
+        if dist_on:
+            dist.barrier()
+        total = sum(a.elapsed_time(b) for a, b in ev) / 1000.0
+        if dist_on:
+            t = torch.tensor([total], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            total = float(t.item())
+        return total, launches
+
+    drop_in = m.default_options()  # FP32, texture-model warp, reference summation order
+    clocks = ClockSampler(local)
+    clocks.start()
+    total, launches = timed(drop_in, args.steps, args.warmup, img, F)
+    clk = clocks.stop()
+    per_rank = args.steps / total
+    value = per_rank * world
+    vox_ray = value * V * nv
+
+    # per-kernel device time of one profiled step (graphs bypassed while profiling)
+    ctx.profile_begin()
+    step(drop_in, img, F)
+    prof = ctx.profile_end()
+    kernel_ms = {k: v[1] for k, v in prof.items()}
+    tot_ms = sum(kernel_ms.values())
+    top = max(prof, key=lambda k: prof[k][1])
+    abytes = algorithmic_bytes(p)
+    peaks = measured_peaks()
+    top_launch_ms = prof[top][1] / prof[top][0]
+    achieved = abytes.get(top, 0) / (top_launch_ms / 1000.0) / 1e9
+    roofline = {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peaks["hbm_gbs"],
+                "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": None,
+                "peak_source": peaks["source"], "launch_ms": top_launch_ms,
+                "algorithmic_bytes_per_launch": abytes.get(top, 0),
+                "share": {k: round(v / tot_ms, 4) for k, v in kernel_ms.items()}}
+
+    # end to end through the host-pointer entry point (host_AUMISART's interface)
+    pin = lambda a: torch.as_tensor(np.ascontiguousarray(a)).pin_memory().numpy()
+    h_img = pin(np.zeros((g["nz"], g["ny"], g["nx"]), np.float32))
+    h_proj = pin(proj.cpu().numpy())
+    h_fields = [pin(f.cpu().numpy()) for f in fields]
+    o_img, o_ax = pin(np.zeros_like(h_img)), pin(np.zeros_like(h_img))
+    o_proj = pin(np.zeros((nv, g["nb"], g["na"]), np.float32))
+    o_norm = pin(np.zeros(2 * nv, np.float32))
+    errw = np.zeros(nv, np.float32)
+
+    def e2e_step():
+        ctx.host_AUMISART(o_img, o_proj, o_norm, o_ax, h_img, h_proj, g["nx"], g["ny"], g["nz"],
+                          g["na"], g["nb"], 1, nv, 2, op, g["da"], g["db"], g["ai"], g["bi"],
+                          g["SO"], g["SD"], 1.0, p.cfg.lam, p.volumes, p.flows, errw, p.angles,
+                          *h_fields)
+
+    for _ in range(max(1, args.warmup)):
+        e2e_step()
+    torch.cuda.synchronize()
+    if dist_on:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_step()
+    e2e_total = time.perf_counter() - t0
+    if dist_on:
+        t = torch.tensor([e2e_total], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_total = float(t.item())
+    e2e = {"value": args.steps / e2e_total * world, "unit": "iterations/s",
+           "h2d_bytes_per_step": int(h_img.nbytes + h_proj.nbytes + 6 * h_img.nbytes),
+           "d2h_bytes_per_step": int(o_img.nbytes + o_proj.nbytes + o_norm.nbytes + o_ax.nbytes),
+           "api": "mcsart_aumisart (host pointers, pinned)"}
+
+    extras = {}
+    if not args.no_extras:
+        for name, kw in (("fast_f32", dict(fp_sum=2)),
+                         ("mixed_bf16", dict(storage=m.BF16, interp=m.INTERP_EXACT, fp_sum=2)),
+                         ("mixed_f16", dict(storage=m.F16, interp=m.INTERP_EXACT, fp_sum=2))):
+            o = m.default_options(**kw)
+            if o.storage == m.F32:
+                pr, Ft = proj, F0.clone()
+            else:
+                dt = torch.bfloat16 if o.storage == m.BF16 else torch.float16
+                pr, Ft = proj.to(dt), F0.to(dt)
+            img2 = torch.zeros_like(img)
+
+            def st(o=o, pr=pr, Ft=Ft, img2=img2):
+                ctx.aumisart_device(geo=g, n_views=nv, lambda_=p.cfg.lam, angles=p.angles,
+                                    volumes=p.volumes, flows=p.flows, img=img2, proj=pr,
+                                    fields=Ft, resid=resid, norm=norm, n_iter=2, op_iter=op,
+                                    options=o)
+            for _ in range(2):
+                st()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(args.steps):
+                st()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            extras[name] = {"value": args.steps / (e0.elapsed_time(e1) / 1000.0) * world,
+                            "unit": "iterations/s"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = cpu_threads()
+        h_proj_np = proj.cpu().numpy()
+        views = args.cpu_views or 8
+        dt, rate, views = cpu_sample(p, h_proj_np, views, threads)
+        cpu = {"value": rate, "unit": "iterations/s", "cores": threads, "kind": "port",
+               "sample": f"{views} views of the image pass + {views - 1} of the DVF-update "
+                         f"pass ({dt:.1f} s), extrapolated to {nv} + {nv - 1} views"}
+
+    if rank == 0:
+        line = {"metric": "McSART iterations/s", "value": value, "unit": "iterations/s",
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": 1000.0 * total / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": config_dict(p, args), "voxel_ray_updates_per_s": vox_ray,
+                "e2e": e2e, "gpu_launches": int(launches), "roofline": roofline,
+                "cpu_baseline": cpu, "clocks": clk, "kernel_ms_per_step": kernel_ms,
+                "extras": extras}
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist_on:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

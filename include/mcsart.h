@@ -1,0 +1,199 @@
+/* mcsart.h - C ABI of the B200-native McSART engine (libmcsart.so).
+ *
+ * Motion-compensated SART cone-beam CT reconstruction with the 5DCT breathing
+ * model d(x,t) = a(t) v(x) + b(t) f(x), as in bill52547/McSART ("AUMISART").
+ *
+ * Every kernel-level entry point replaces one reference launcher and keeps its
+ * argument meaning and order; the reference file:line is given beside each.
+ * Differences from the reference at this boundary:
+ *   - a context argument comes first (stream, workspaces, cached graphs);
+ *   - every function returns an int status (MCSART_OK or a negative code) and
+ *     mcsart_last_error() describes the failure (the reference returns void and
+ *     checks nothing);
+ *   - work is stream-ordered on the context's stream; call mcsart_synchronize
+ *     (or set synchronous mode) where the reference relied on its
+ *     cudaDeviceSynchronize after every launch.
+ *
+ * Layouts are the reference's: volumes img[ix + iy*nx + iz*nx*ny] (MATLAB
+ * nx x ny x nz), projections proj[ia + ib*na (+ v*na*nb)].  Geometry is in voxel
+ * units (SO = SAD/dx, SD = SDD/dx, da = pitch_a/dx, db = pitch_b/dx) with ai,
+ * bi already shifted by -(n/2 - 0.5) (src/entry_AUMISART.cu:76-94).
+ * Pointers named d_* are device pointers, h_* host pointers.
+ */
+#ifndef MCSART_H
+#define MCSART_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MCSART_VERSION 10000 /* 1.0.0 */
+
+/* status codes */
+#define MCSART_OK 0
+#define MCSART_ERR_INVALID_ARGUMENT (-1)
+#define MCSART_ERR_CUDA (-2)
+#define MCSART_ERR_NO_DEVICE (-3)
+#define MCSART_ERR_OUT_OF_MEMORY (-4)
+#define MCSART_ERR_UNSUPPORTED (-5)
+
+/* storage types of volumes, DVF fields and projections in the engine's own
+ * driver (arithmetic is FP32 in every mode) */
+typedef enum { MCSART_F32 = 0, MCSART_BF16 = 1, MCSART_F16 = 2 } mcsart_dtype;
+
+/* trilinear interpolation model of the warp */
+typedef enum {
+    /* the reference's hardware linear texture filtering: fractional weights
+     * carried with 8 bits (src/cu_deform.cu:29-38,89) */
+    MCSART_INTERP_TEXTURE = 0,
+    /* full FP32 trilinear weights */
+    MCSART_INTERP_EXACT = 1
+} mcsart_interp;
+
+typedef struct mcsart_ctx mcsart_ctx;
+
+/* ------------------------------------------------------------- context */
+int mcsart_version(void);
+/* Description of the last failure on the calling thread ("" if none). */
+const char *mcsart_last_error(void);
+/* Create a context on CUDA device `device` with its own non-blocking stream. */
+int mcsart_create(mcsart_ctx **ctx, int device);
+int mcsart_destroy(mcsart_ctx *ctx);
+/* Enqueue on an external cudaStream_t from now on; NULL selects the legacy
+ * default stream (the one torch uses unless told otherwise).  A new context
+ * starts on its own non-blocking stream. */
+int mcsart_set_stream(mcsart_ctx *ctx, void *cuda_stream);
+void *mcsart_get_stream(mcsart_ctx *ctx);
+/* Non-zero: every entry point synchronises before returning (reference
+ * behaviour, src/cu_*.cu call cudaDeviceSynchronize after each launch). */
+int mcsart_set_synchronous(mcsart_ctx *ctx, int on);
+int mcsart_synchronize(mcsart_ctx *ctx);
+/* Warp model for mcsart_deform and the drivers (default TEXTURE). */
+int mcsart_set_interp(mcsart_ctx *ctx, int interp);
+/* Number of this library's kernels launched through ctx so far. */
+long long mcsart_launch_count(mcsart_ctx *ctx);
+/* Per-kernel timing: between begin and end every launch is bracketed by CUDA
+ * events on the context stream (CUDA graphs are bypassed meanwhile); end
+ * synchronises and fills a table of (kernel name, launches, total ms). */
+int mcsart_profile_begin(mcsart_ctx *ctx);
+int mcsart_profile_end(mcsart_ctx *ctx);
+int mcsart_profile_count(mcsart_ctx *ctx);
+int mcsart_profile_entry(mcsart_ctx *ctx, int i, char *name, int name_len, long long *launches,
+                         double *total_ms);
+
+/* ------------------------------------------------- kernel-level (device) */
+/* replaces host_projection, include/cu_projection.h:7 (src/cu_projection.cu:7) */
+int mcsart_projection(mcsart_ctx *ctx, float *d_proj, const float *d_img, float angle, float SO,
+                      float SD, float da, int na, float ai, float db, int nb, float bi, int nx,
+                      int ny, int nz);
+/* replaces host_backprojection, include/cu_backprojection.h:7 (src/cu_backprojection.cu:8) */
+int mcsart_backprojection(mcsart_ctx *ctx, float *d_img, const float *d_proj, float angle,
+                          float SO, float SD, float da, int na, float ai, float db, int nb,
+                          float bi, int nx, int ny, int nz);
+/* replaces host_deform, include/cu_deform.h:8 (src/cu_deform.cu:3); d_img1 may
+ * equal d_img */
+int mcsart_deform(mcsart_ctx *ctx, float *d_img1, const float *d_img, int nx, int ny, int nz,
+                  float volume, float flow, const float *alpha_x, const float *alpha_y,
+                  const float *alpha_z, const float *beta_x, const float *beta_y,
+                  const float *beta_z);
+/* replaces host_deform2, include/cu_deform.h:9 (src/cu_deform.cu:49) */
+int mcsart_deform2(mcsart_ctx *ctx, float *d_img1, const float *d_img, int nx, int ny, int nz,
+                   float volume, float flow, const float *alpha_x, const float *alpha_y,
+                   const float *alpha_z, const float *beta_x, const float *beta_y,
+                   const float *beta_z);
+/* replaces kernel_forwardDVF, include/cu_deform.h:10 (src/cu_deform.cu:66) */
+int mcsart_forward_dvf(mcsart_ctx *ctx, float *mx, float *my, float *mz, const float *alpha_x,
+                       const float *alpha_y, const float *alpha_z, const float *beta_x,
+                       const float *beta_y, const float *beta_z, float volume, float flow,
+                       int nx, int ny, int nz);
+/* replaces host_add, include/cu_add.h:4 (src/cu_add.cu:2) */
+int mcsart_add(mcsart_ctx *ctx, float *img1, const float *img, int nx, int ny, int nz,
+               float weight);
+/* replaces host_add2, include/cu_add.h:8 (src/cu_add.cu:20) */
+int mcsart_add2(mcsart_ctx *ctx, float *img1, const float *img, int nx, int ny, int nz,
+                const float *img0, float weight, int ind);
+/* replaces host_initial, include/cu_initial.h:5 (src/cu_initial.cu:2) */
+int mcsart_initial(mcsart_ctx *ctx, float *img, int nx, int ny, int nz, float value);
+/* replaces host_initial2, include/cu_initial.h:8 (src/cu_initial.cu:20) */
+int mcsart_initial2(mcsart_ctx *ctx, float *img, int nx, int ny, int nz, const float *img0,
+                    float volume, float flow);
+/* replaces host_division, include/cu_division.h:5 (src/cu_division.cu:2) */
+int mcsart_division(mcsart_ctx *ctx, float *img1, const float *img, int nx, int ny, int nz);
+/* replaces host_multiple, include/cu_multiple.h:4 (src/cu_multiple.cu:2) */
+int mcsart_multiple(mcsart_ctx *ctx, float *img1, int nx, int ny, int nz, const float *img0,
+                    float weight, int ind);
+/* replaces host_update_udvf, include/cu_update_udvf.h:8 (src/cu_update_udvf.cu:3) */
+int mcsart_update_udvf(mcsart_ctx *ctx, float *alpha_x, float *alpha_y, float *alpha_z,
+                       float *beta_x, float *beta_y, float *beta_z, const float *img,
+                       const float *img0, float volume_diff, float flow_diff, int nx, int ny,
+                       int nz, int iter);
+/* replaces host_diff, src/mex_diff.cu:67 (the mex_diff gateway's kernel) */
+int mcsart_diff(mcsart_ctx *ctx, float *img1, const float *img, int nx, int ny, int nz, int ind);
+/* replaces the cublasSnrm2 calls of src/AUMISART.cu:48,51 (FP64 accumulation);
+ * writes the norm to *h_result after synchronising */
+int mcsart_snrm2(mcsart_ctx *ctx, int n, const float *d_x, float *h_result);
+
+/* ---------------------------------------------------- batched projector */
+/* All n_views views of one volume in a single launch:
+ * d_proj[v*na*nb + ia + ib*na] = FP(d_img, h_angles[v]).  Same operator as
+ * mcsart_projection per view. */
+int mcsart_projection_views(mcsart_ctx *ctx, float *d_proj, const float *d_img,
+                            const float *h_angles, int n_views, float SO, float SD, float da,
+                            int na, float ai, float db, int nb, float bi, int nx, int ny,
+                            int nz);
+
+/* ------------------------------------------------------------ drivers */
+/* replaces host_AUMISART, include/AUMISART.h:17 and :19 (src/AUMISART.cu:3,
+ * :143).  Host pointers, the reference's argument list and order.  If alpha_x
+ * is NULL the DVF starts at zero and the motion pass steps views by 10
+ * (overload 1); otherwise all six fields are read and the motion pass steps
+ * by 1 (overload 2).  Outputs: h_outimg (nx*ny*nz), h_outproj (na*nb*n_views
+ * residuals of the last image pass), h_outnorm (n_iter*n_views ratios
+ * ||b-Ax||/||b||; entries of skipped views are 0), h_outalphax (nx*ny*nz).
+ * err_weights and outIter are accepted and unused, as in the reference. */
+int mcsart_aumisart(mcsart_ctx *ctx, float *h_outimg, float *h_outproj, float *h_outnorm,
+                    float *h_outalphax, const float *h_img, const float *h_proj, int nx, int ny,
+                    int nz, int na, int nb, int outIter, int n_views, int n_iter,
+                    const int *op_iter, float da, float db, float ai, float bi, float SO,
+                    float SD, float dx, float lambda, const float *volumes, const float *flows,
+                    const float *err_weights, const float *angles, const float *alpha_x,
+                    const float *alpha_y, const float *alpha_z, const float *beta_x,
+                    const float *beta_y, const float *beta_z);
+
+/* Engine options for the device-resident driver. */
+typedef struct {
+    int storage;      /* mcsart_dtype of the DVF fields, warped volumes and projections */
+    int interp;       /* mcsart_interp */
+    int use_graph;    /* capture each pass as a CUDA graph and replay it */
+    int fp_sum;       /* projector ray sums: 0 = the reference's order, one thread per
+                         ray (bitwise drop-in); 1 = per-slab partial sums, slabs split
+                         across warps; 2 = as 1 with Kahan-compensated slab sums */
+    int fp_groups;    /* slab groups per ray in modes 1 and 2 (0 = auto) */
+} mcsart_options;
+void mcsart_default_options(mcsart_options *opt);
+
+/* One reconstruction problem with device-resident state. */
+typedef struct {
+    int nx, ny, nz, na, nb, n_views;
+    float SO, SD, da, db, ai, bi, lambda;
+    const float *h_angles;   /* n_views, radians */
+    const float *h_volumes;  /* n_views, a(t_v) */
+    const float *h_flows;    /* n_views, b(t_v) */
+    float *d_img;            /* in/out, FP32 volume */
+    const void *d_proj;      /* measured projections, storage dtype, n_views*na*nb */
+    void *d_fields;          /* 6*nx*ny*nz (ax,ay,az,bx,by,bz), storage dtype; NULL = overload 1 */
+    float *d_resid;          /* optional out: residuals of the last image pass, FP32 */
+    float *d_norm;           /* optional out: n_iter*n_views norm ratios, FP32 */
+} mcsart_problem;
+
+/* Run n_iter outer iterations (op_iter[i]==1: image pass, else motion pass)
+ * of host_AUMISART's loop on device-resident buffers. */
+int mcsart_aumisart_device(mcsart_ctx *ctx, const mcsart_problem *prob, int n_iter,
+                           const int *h_op_iter, const mcsart_options *opt);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MCSART_H */

@@ -1,0 +1,199 @@
+// Internal definitions shared by the engine's translation units.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <memory>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "mcsart.h"
+
+namespace mcsart {
+
+// ------------------------------------------------------------------ errors
+void set_error(const char *fmt, ...);
+void clear_error();
+
+#define MC_CHECK_CUDA(expr)                                                                     \
+    do {                                                                                        \
+        cudaError_t e_ = (expr);                                                                \
+        if (e_ != cudaSuccess) {                                                                \
+            ::mcsart::set_error("%s: %s (%s:%d)", #expr, cudaGetErrorString(e_), __FILE__,      \
+                                __LINE__);                                                      \
+            return MCSART_ERR_CUDA;                                                             \
+        }                                                                                       \
+    } while (0)
+
+#define MC_REQUIRE(cond, ...)                                                                   \
+    do {                                                                                        \
+        if (!(cond)) {                                                                          \
+            ::mcsart::set_error(__VA_ARGS__);                                                   \
+            return MCSART_ERR_INVALID_ARGUMENT;                                                 \
+        }                                                                                       \
+    } while (0)
+
+#define MC_TRY(expr)                                                                            \
+    do {                                                                                        \
+        int rc_ = (expr);                                                                       \
+        if (rc_ != MCSART_OK) return rc_;                                                       \
+    } while (0)
+
+// Status after a kernel launch (configuration errors surface here).
+int check_launch(const char *what);
+
+struct DriverState;  // sart.cu
+
+}  // namespace mcsart
+
+struct mcsart_ctx {
+    // per-kernel timing (mcsart_profile_begin/end): events around each launch
+    struct ProfRec {
+        const char *name;
+        cudaEvent_t e0, e1;
+    };
+    struct ProfAgg {
+        long long launches = 0;
+        double ms = 0.0;
+    };
+    bool profiling = false;
+    const char *label = nullptr;  // name of the next launch (else the kernel expression)
+    std::vector<ProfRec> prof_pending;
+    std::vector<cudaEvent_t> prof_pool;
+    std::vector<std::pair<std::string, ProfAgg>> prof_table;
+    int device = 0;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    int synchronous = 0;
+    int interp = MCSART_INTERP_TEXTURE;
+    long long launches = 0;
+    struct Buf {
+        void *ptr = nullptr;
+        size_t bytes = 0;
+    };
+    std::map<std::string, Buf> ws;  // named device workspaces, grown on demand
+    std::unique_ptr<mcsart::DriverState> driver;
+    ~mcsart_ctx();
+};
+
+namespace mcsart {
+
+// Device workspace `name` of at least `bytes` (contents undefined).
+int workspace(mcsart_ctx *ctx, const char *name, size_t bytes, void **out);
+// Called after enqueuing work: synchronises in synchronous mode.
+int finish(mcsart_ctx *ctx, const char *what);
+int validate_ctx(mcsart_ctx *ctx);
+
+// ------------------------------------------------------------ geometry
+struct Geom {
+    float SO, SD, da, ai, db, bi;
+    int na, nb, nx, ny, nz;
+};
+
+__host__ __device__ inline int64_t nvox(int nx, int ny, int nz) { return (int64_t)nx * ny * nz; }
+
+int validate_geom(const Geom &g);
+int validate_dims(int nx, int ny, int nz);
+
+// -------------------------------------------------------- storage types
+template <typename T> __device__ __forceinline__ float ldv(const T *p, int64_t i);
+template <> __device__ __forceinline__ float ldv<float>(const float *p, int64_t i) {
+    return __ldg(p + i);
+}
+template <> __device__ __forceinline__ float ldv<__nv_bfloat16>(const __nv_bfloat16 *p, int64_t i) {
+    return __bfloat162float(p[i]);
+}
+template <> __device__ __forceinline__ float ldv<__half>(const __half *p, int64_t i) {
+    return __half2float(p[i]);
+}
+template <typename T> __device__ __forceinline__ T cvt(float v);
+template <> __device__ __forceinline__ float cvt<float>(float v) { return v; }
+template <> __device__ __forceinline__ __nv_bfloat16 cvt<__nv_bfloat16>(float v) {
+    return __float2bfloat16_rn(v);
+}
+template <> __device__ __forceinline__ __half cvt<__half>(float v) { return __float2half_rn(v); }
+
+// ------------------------------------------------- trilinear sampling
+// Source of a trilinear gather.  SrcTex samples a 3D texture with hardware
+// linear filtering and clamp addressing, exactly the configuration the
+// reference builds for its warp (src/cu_deform.cu:25-38); SrcLinear samples
+// a linear x-fastest volume in software with full FP32 weights (the EXACT
+// model).  Coordinates are unnormalised texture coordinates (texel centres at
+// i + 0.5).
+struct SrcTex {
+    cudaTextureObject_t tex;
+    __device__ __forceinline__ float fetch(float x, float y, float z, int, int, int) const {
+        return tex3D<float>(tex, x, y, z);
+    }
+};
+
+__device__ __forceinline__ void lin_axis(float x, int n, int &i0, int &i1, float &w) {
+    const float xb = x - 0.5f;
+    const float fl = floorf(xb);
+    w = xb - fl;
+    // clamp in float first so that far-out coordinates cannot overflow the conversion
+    const int i = (int)fminf(fmaxf(fl, -1.0f), (float)n);
+    i0 = min(max(i, 0), n - 1);
+    i1 = min(max(i + 1, 0), n - 1);
+}
+
+template <typename T> struct SrcLinear {
+    const T *p;
+    __device__ __forceinline__ float fetch(float x, float y, float z, int nx, int ny,
+                                           int nz) const {
+        int x0, x1, y0, y1, z0, z1;
+        float a, b, c;
+        lin_axis(x, nx, x0, x1, a);
+        lin_axis(y, ny, y0, y1, b);
+        lin_axis(z, nz, z0, z1, c);
+        const int64_t sy = nx, sz = (int64_t)nx * ny;
+        const int64_t r00 = y0 * sy + z0 * sz, r10 = y1 * sy + z0 * sz;
+        const int64_t r01 = y0 * sy + z1 * sz, r11 = y1 * sy + z1 * sz;
+        const float t000 = ldv(p, x0 + r00), t100 = ldv(p, x1 + r00);
+        const float t010 = ldv(p, x0 + r10), t110 = ldv(p, x1 + r10);
+        const float t001 = ldv(p, x0 + r01), t101 = ldv(p, x1 + r01);
+        const float t011 = ldv(p, x0 + r11), t111 = ldv(p, x1 + r11);
+        // lerps along x, then y, then z
+        const float c00 = fmaf(a, t100 - t000, t000), c10 = fmaf(a, t110 - t010, t010);
+        const float c01 = fmaf(a, t101 - t001, t001), c11 = fmaf(a, t111 - t011, t011);
+        const float c0 = fmaf(b, c10 - c00, c00), c1 = fmaf(b, c11 - c01, c01);
+        return fmaf(c, c1 - c0, c0);
+    }
+};
+
+// 3D array with texture (linear filtering, clamp) and surface views, used as
+// the source of hardware-filtered warps.
+struct TexVol {
+    cudaArray_t arr = nullptr;
+    cudaTextureObject_t tex = 0;
+    cudaSurfaceObject_t surf = 0;
+    int nx = 0, ny = 0, nz = 0;
+    int ensure(int nx, int ny, int nz);
+    int upload(const float *src, cudaStream_t st);  // linear x-fastest volume -> array
+    void release();
+    ~TexVol() { release(); }
+};
+
+// Counted launch on the context stream.
+int prof_before(mcsart_ctx *ctx, const char *name);
+int prof_after(mcsart_ctx *ctx);
+
+// Counted (and, while profiling, event-timed) launch on the context stream.
+#define MC_LAUNCH(ctx, kernel, grid, block, smem, ...)                                          \
+    do {                                                                                        \
+        if ((ctx)->profiling) MC_TRY(::mcsart::prof_before((ctx), #kernel));                    \
+        kernel<<<(grid), (block), (smem), (ctx)->stream>>>(__VA_ARGS__);                        \
+        (ctx)->launches++;                                                                      \
+        MC_TRY(::mcsart::check_launch(#kernel));                                                \
+        if ((ctx)->profiling) MC_TRY(::mcsart::prof_after(ctx));                                \
+        (ctx)->label = nullptr;                                                                 \
+    } while (0)
+
+inline unsigned div_up(int64_t a, int64_t b) { return (unsigned)((a + b - 1) / b); }
+
+}  // namespace mcsart

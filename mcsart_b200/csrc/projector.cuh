@@ -1,0 +1,285 @@
+// Distance-driven forward projector (the reference's kernel_projection,
+// src/cu_projection.cu:15-145), restructured for B200.
+//
+// Reference semantics kept exactly: per-ray driving axis |x21| > |y21| (:39);
+// the four in-plane edge ratios yl/xl, yl/xr, yr/xl, yr/xr and their min/max
+// (:54-64); axial edges zl/x21, zr/x21 (:71-77); integer ny/2, nz/2 offsets
+// against float nx/2 (:52,55,72); overlap weights normalised by the footprint
+// width (:83,86); loops clamped to the volume.
+//
+// Restructured for the hardware:
+//   * one thread per ray (the reference runs 4 redundant threads per ray that
+//     race on a non-atomic +=);
+//   * the slabs of a ray are split across `groups` warps of a block and
+//     recombined in a fixed order through shared memory (deterministic);
+//   * the loop-invariant ratios are hoisted out of the slab loop;
+//   * x-driven rays read a y-fastest copy of the volume so that the 32 lanes
+//     of a warp (adjacent detector columns) gather adjacent addresses;
+//   * up to three volumes are projected with one set of weights, the
+//     projection of a ones-volume (sum of weights) comes for free, and the
+//     SART residual, its norm partial sums and the packing for the
+//     backprojector are done in the epilogue.
+#pragma once
+
+#include "common.cuh"
+
+namespace mcsart {
+
+enum FPMode { FP_PLAIN = 0, FP_IMAGE = 1, FP_MOTION = 2 };
+
+struct RayGeom {
+    float r0, r1, r2, r3;  // in-plane edge ratios
+    float rz0, rz1;        // axial edge ratios
+    float u_off;           // source coordinate along the in-plane axis (y1 or x1)
+    float u_half;          // (float)(nu/2), integer division
+    float d_half;          // (float)nd/2, float division
+    float src_d;           // source coordinate along the driving axis (x1 or y1)
+    int nd, nu;
+    bool xdrive;
+};
+
+// src/cu_projection.cu:23-39,48-51,67-68,101-104,120-121 for ray (ia, ib).
+__device__ __forceinline__ RayGeom ray_geom(float cphi, float sphi, int ia, int ib,
+                                            const Geom &g) {
+    const float x1 = -g.SO * cphi, y1 = -g.SO * sphi, z1 = 0.0f;
+    const float x20 = g.SD - g.SO;
+    const float y20 = (ia + g.ai) * g.da;
+    const float x2 = x20 * cphi - y20 * sphi;
+    const float y2 = x20 * sphi + y20 * cphi;
+    const float z2 = (ib + g.bi) * g.db;
+    const float x21 = x2 - x1, y21 = y2 - y1, z21 = z2 - z1;
+    RayGeom r;
+    r.xdrive = fabsf(x21) > fabsf(y21);
+    const float xl = x21 - g.da / 2 * sphi, xr = x21 + g.da / 2 * sphi;
+    const float yl = y21 - g.da / 2 * cphi, yr = y21 + g.da / 2 * cphi;
+    const float zl = z21 - g.db / 2, zr = z21 + g.db / 2;
+    if (r.xdrive) {
+        r.r0 = yl / xl; r.r1 = yl / xr; r.r2 = yr / xl; r.r3 = yr / xr;
+        r.rz0 = zl / x21; r.rz1 = zr / x21;
+        r.u_off = y1; r.u_half = (float)(g.ny / 2);
+        r.d_half = (float)g.nx / 2; r.src_d = x1;
+        r.nd = g.nx; r.nu = g.ny;
+    } else {
+        r.r0 = xl / yl; r.r1 = xl / yr; r.r2 = xr / yl; r.r3 = xr / yr;
+        r.rz0 = zl / y21; r.rz1 = zr / y21;
+        r.u_off = x1; r.u_half = (float)(g.nx / 2);
+        r.d_half = (float)g.ny / 2; r.src_d = y1;
+        r.nd = g.ny; r.nu = g.nx;
+    }
+    return r;
+}
+
+template <typename VT, int K> struct FPVolumes {
+    const VT *std[K];  // x-fastest volumes
+    const VT *tr[K];   // y-fastest copies (tr[k][iy + ix*ny + iz*nx*ny]) or nullptr
+};
+
+// Ray-sum order.  SUM_REF accumulates every voxel term straight into the ray
+// sum in the reference's order (slabs, then in-plane, then axial index,
+// acc = fma(v*w_u, w_z, acc), cu_projection.cu:81-88), so that results are
+// bitwise those of the reference kernel.  SUM_PLAIN / SUM_KAHAN first sum the
+// (at most a few) terms of one slab and then add the slab sum to the ray sum,
+// plainly or with Kahan compensation; they allow the slabs of a ray to be
+// split across warps.
+enum SumMode { SUM_REF = 0, SUM_PLAIN = 1, SUM_KAHAN = 2 };
+
+// Accumulates the footprint of slabs [d0, d1) of one ray into s[0..K-1]
+// (volume sums) and sw (sum of weights = projection of a ones-volume).
+template <int K, bool ONES, int SUM, typename VT>
+__device__ __forceinline__ void ray_slabs(const RayGeom &r, const FPVolumes<VT, K> &v,
+                                          const Geom &g, int d0, int d1, float *s, float &sw) {
+    const VT *base[K];
+    int64_t su, sd;
+    const int64_t sz = (int64_t)g.nx * g.ny;
+    if (r.xdrive) {
+        if (v.tr[0] != nullptr) {
+#pragma unroll
+            for (int k = 0; k < K; k++) base[k] = v.tr[k];
+            su = 1; sd = g.ny;
+        } else {
+#pragma unroll
+            for (int k = 0; k < K; k++) base[k] = v.std[k];
+            su = g.nx; sd = 1;
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < K; k++) base[k] = v.std[k];
+        su = 1; sd = g.nx;
+    }
+    const float z_half = (float)(g.nz / 2);
+    float acc[K], cmp[K], accw = 0.0f, cmpw = 0.0f;
+#pragma unroll
+    for (int k = 0; k < K; k++) { acc[k] = 0.0f; cmp[k] = 0.0f; }
+
+    for (int d = d0; d < d1; d++) {
+        // :52 / :105
+        const float dc = __fsub_rn(__fsub_rn(__fadd_rn((float)d, 0.5f), r.d_half), r.src_d);
+        // :54-61 / :107-114 ("ratio * xc + y1 + ny / 2")
+        const float c0 = __fadd_rn(__fmaf_rn(r.r0, dc, r.u_off), r.u_half);
+        const float c1 = __fadd_rn(__fmaf_rn(r.r1, dc, r.u_off), r.u_half);
+        const float c2 = __fadd_rn(__fmaf_rn(r.r2, dc, r.u_off), r.u_half);
+        const float c3 = __fadd_rn(__fmaf_rn(r.r3, dc, r.u_off), r.u_half);
+        const float ui1 = fminf(fminf(c0, c1), fminf(c2, c3));
+        const float ui2 = fmaxf(fmaxf(c0, c1), fmaxf(c2, c3));
+        // :71-77 / :124-130 ("ratio * xc + z1 + nz / 2", z1 = 0)
+        const float cz0 = __fadd_rn(__fmul_rn(r.rz0, dc), z_half);
+        const float cz1 = __fadd_rn(__fmul_rn(r.rz1, dc), z_half);
+        const float zi1 = fminf(cz0, cz1), zi2 = fmaxf(cz0, cz1);
+        const int u_lo = max(0, (int)floorf(ui1)), u_hi = min(r.nu - 1, (int)floorf(ui2));
+        const int z_lo = max(0, (int)floorf(zi1)), z_hi = min(g.nz - 1, (int)floorf(zi2));
+        if (u_lo > u_hi || z_lo > z_hi) continue;
+        const float du = ui2 - ui1, dz = zi2 - zi1;
+        float ss[K], ssw = 0.0f;
+#pragma unroll
+        for (int k = 0; k < K; k++) ss[k] = 0.0f;
+        for (int u = u_lo; u <= u_hi; u++) {
+            // :83 / :136
+            const float wu = __fdiv_rn(fminf(u + 1.0f, ui2) - fmaxf(u + 0.0f, ui1), du);
+            const int64_t row = (int64_t)u * su + (int64_t)d * sd;
+            for (int z = z_lo; z <= z_hi; z++) {
+                // :86 / :139
+                const float wz = __fdiv_rn(fminf(z + 1.0f, zi2) - fmaxf(z + 0.0f, zi1), dz);
+                const int64_t a = row + (int64_t)z * sz;
+                if (SUM == SUM_REF) {
+#pragma unroll
+                    for (int k = 0; k < K; k++)
+                        acc[k] = __fmaf_rn(ldv(base[k], a) * wu, wz, acc[k]);  // :87 / :140
+                    if (ONES) accw = __fmaf_rn(wu, wz, accw);
+                } else {
+#pragma unroll
+                    for (int k = 0; k < K; k++) ss[k] = __fmaf_rn(ldv(base[k], a) * wu, wz, ss[k]);
+                    if (ONES) ssw = __fmaf_rn(wu, wz, ssw);
+                }
+            }
+        }
+        if (SUM == SUM_REF) continue;
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            if (SUM == SUM_KAHAN) {
+                const float y = ss[k] - cmp[k];
+                const float t = acc[k] + y;
+                cmp[k] = (t - acc[k]) - y;
+                acc[k] = t;
+            } else {
+                acc[k] += ss[k];
+            }
+        }
+        if (ONES) {
+            if (SUM == SUM_KAHAN) {
+                const float y = ssw - cmpw;
+                const float t = accw + y;
+                cmpw = (t - accw) - y;
+                accw = t;
+            } else {
+                accw += ssw;
+            }
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < K; k++) s[k] = acc[k];
+    sw = accw;
+}
+
+template <typename VT, int K, typename MT = VT> struct FPArgs {
+    FPVolumes<VT, K> vol;
+    Geom g;
+    float angle;            // used when angles == nullptr
+    const float *angles;    // per-view angles (device), view = blockIdx.z
+    int mode;
+    // FP_PLAIN: out[view*na*nb + ia + ib*na] = s0
+    float *out;
+    // FP_IMAGE / FP_MOTION
+    const MT *meas;     // measured projection of this view
+    float *resid;       // residual output (nullable)
+    float2 *bp_in;      // (residual, ones-projection) pairs for the backprojector
+    double2 *norm_part; // per-block (sum b^2, sum r^2)
+};
+
+// Launch shapes.  SUM_REF: blockDim (32, 8), one ray per thread, 32 columns x
+// 8 rows per block, gridDim (ceil(na/32), ceil(nb/8), views).  Split modes:
+// blockDim (32, groups), threadIdx.y = slab group of the same 32 rays,
+// gridDim (ceil(na/32), nb, views).
+template <int K, bool ONES, int SUM, typename VT, typename MT = VT>
+__global__ void __launch_bounds__(256) fp_kernel(const FPArgs<VT, K, MT> p) {
+    constexpr int NS = K + (ONES ? 1 : 0);
+    extern __shared__ float sm_fp[];  // split modes: [groups][NS][32]
+    __shared__ double2 sm_norm[8];
+    const int lane = threadIdx.x;
+    const Geom &g = p.g;
+    const int ia = blockIdx.x * 32 + lane;
+    const int ib = (SUM == SUM_REF) ? blockIdx.y * 8 + threadIdx.y : blockIdx.y;
+    const bool active = ia < g.na && ib < g.nb;
+    float s[K], sw = 0.0f;
+#pragma unroll
+    for (int k = 0; k < K; k++) s[k] = 0.0f;
+    if (active) {
+        const float angle = p.angles ? p.angles[blockIdx.z] : p.angle;
+        const float cphi = cosf(angle), sphi = sinf(angle);  // :23-24
+        const RayGeom r = ray_geom(cphi, sphi, ia, ib, g);
+        if (SUM == SUM_REF) {
+            ray_slabs<K, ONES, SUM, VT>(r, p.vol, g, 0, r.nd, s, sw);
+        } else {
+            const int groups = blockDim.y, grp = threadIdx.y;
+            const int per = (r.nd + groups - 1) / groups;
+            const int d0 = grp * per, d1 = min(r.nd, d0 + per);
+            ray_slabs<K, ONES, SUM, VT>(r, p.vol, g, d0, d1, s, sw);
+        }
+    }
+    if (SUM != SUM_REF) {
+        const int grp = threadIdx.y, groups = blockDim.y;
+#pragma unroll
+        for (int k = 0; k < K; k++) sm_fp[(grp * NS + k) * 32 + lane] = s[k];
+        if (ONES) sm_fp[(grp * NS + K) * 32 + lane] = sw;
+        __syncthreads();
+        if (grp != 0) return;
+        // fixed-order combination of the slab groups
+        for (int q = 1; q < groups; q++) {
+#pragma unroll
+            for (int k = 0; k < K; k++) s[k] += sm_fp[(q * NS + k) * 32 + lane];
+            if (ONES) sw += sm_fp[(q * NS + K) * 32 + lane];
+        }
+    }
+    const int64_t pix = ia + (int64_t)ib * g.na;
+    double nb2 = 0.0, nr2 = 0.0;
+    if (active) {
+        if (p.mode == FP_PLAIN) {
+            p.out[pix + (int64_t)blockIdx.z * g.na * g.nb] = s[0];
+        } else {
+            const float b = ldv(p.meas, pix);
+            // AUMISART.cu:206 host_add(proj, proj_temp, -1): proj += proj_temp * -1
+            float res = __fmaf_rn(s[0], -1.0f, b);
+            float ones = ONES ? sw : 0.0f;
+            if (p.mode == FP_MOTION) {
+                res = __fmaf_rn(s[1], 1.0f, res);  // AUMISART.cu:260, + FP(img0)
+                if (K >= 3) ones = s[2];            // FP(initial2(...)), :267-268
+            }
+            if (p.resid) p.resid[pix] = res;
+            p.bp_in[pix] = make_float2(res, ones);
+            nb2 = (double)b * (double)b;
+            nr2 = (double)res * (double)res;
+        }
+    }
+    if (p.mode == FP_PLAIN) return;
+    // block partial of the two squared norms, fixed-order reduction
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        nb2 += __shfl_down_sync(0xffffffffu, nb2, off);
+        nr2 += __shfl_down_sync(0xffffffffu, nr2, off);
+    }
+    if (SUM != SUM_REF) {  // only warp 0 is left
+        if (lane == 0) p.norm_part[blockIdx.y * gridDim.x + blockIdx.x] = make_double2(nb2, nr2);
+        return;
+    }
+    if (lane == 0) sm_norm[threadIdx.y] = make_double2(nb2, nr2);
+    __syncthreads();
+    if (threadIdx.y == 0 && lane == 0) {
+        double tb = 0.0, tr = 0.0;
+        for (int w = 0; w < (int)blockDim.y; w++) {
+            tb += sm_norm[w].x;
+            tr += sm_norm[w].y;
+        }
+        p.norm_part[blockIdx.y * gridDim.x + blockIdx.x] = make_double2(tb, tr);
+    }
+}
+
+}  // namespace mcsart

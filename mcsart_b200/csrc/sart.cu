@@ -1,0 +1,556 @@
+// The SART / motion driver: replacement of host_AUMISART (src/AUMISART.cu:3-313).
+//
+// Per view the reference launches ~20 kernels, each followed by
+// cudaDeviceSynchronize, allocates a cudaArray in every backprojection and
+// warp, calls cublasSnrm2 twice in host-pointer mode and copies the measured
+// projection H2D and the residual D2H.  Here every pass over the views is a
+// fixed sequence of fused kernels on device-resident buffers:
+//
+//   image pass, static (overload 1, AUMISART.cu:42-63):
+//     FP(img) + FP(ones) + residual + norms  ->  BP(residual)/BP(FP(ones)),
+//     img += lambda * ratio (and its y-fastest copy)            2 kernels/view
+//   image pass, motion-compensated (overload 2, :184-233):
+//     warp(img) -> FP + FP(ones) + residual + norms -> BP ratio ->
+//     img += lambda * warp^-1(ratio)                            4 kernels/view
+//   motion pass (:66-118 / :236-288):
+//     img0 and initial2 volumes -> FP of img, img0, ones + residual + norms ->
+//     BP ratio -> six field updates                             4 kernels/view
+//
+// The sequence of a pass is captured once as a CUDA graph and replayed for
+// every outer iteration of that kind.
+#include <cstring>
+#include <vector>
+
+#include "backprojector.cuh"
+#include "common.cuh"
+#include "elementwise.cuh"
+#include "projector.cuh"
+#include "sart.cuh"
+#include "warp.cuh"
+
+#define MC_EXPORT extern "C" __attribute__((visibility("default")))
+
+namespace mcsart {
+
+int fp_auto_groups(int64_t ray_blocks, int n_slabs);
+unsigned stream_blocks(int64_t n);
+
+int DevBuf::ensure(size_t n) {
+    if (bytes >= n && ptr) return MCSART_OK;
+    release();
+    const cudaError_t e = cudaMalloc(&ptr, n ? n : 1);
+    if (e != cudaSuccess) {
+        ptr = nullptr;
+        set_error("device allocation of %zu bytes failed: %s", n, cudaGetErrorString(e));
+        return e == cudaErrorMemoryAllocation ? MCSART_ERR_OUT_OF_MEMORY : MCSART_ERR_CUDA;
+    }
+    bytes = n;
+    return MCSART_OK;
+}
+
+void DevBuf::release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+}
+
+void PassGraph::release() {
+    if (exec) cudaGraphExecDestroy(exec);
+    exec = nullptr;
+    key.clear();
+    kernels = 0;
+}
+
+enum PassKind { PASS_IMAGE_STATIC = 1, PASS_IMAGE_MC = 2, PASS_MOTION = 3 };
+
+struct Problem {
+    Geom g;
+    int n_views;
+    float lambda;
+    const float *angles, *volumes, *flows;  // host, n_views each
+    float *img;                             // device, FP32
+    const void *proj;                       // device, storage type, n_views*na*nb
+    void *fields;                           // device, storage type, 6 volumes
+    bool motion_model;                      // overload 2
+    float *resid;                           // device FP32 or nullptr
+};
+
+template <typename ST, int INTERP, int SUM> struct Runner {
+    mcsart_ctx *ctx;
+    DriverState &S;
+    const Problem &P;
+    const mcsart_options &opt;
+    int64_t V = 0, NP = 0;
+    int fp_bx = 0, fp_by = 0, fp_blocks = 0, groups = 1;
+    std::vector<int> views_img, views_mot;
+
+    Runner(mcsart_ctx *c, const Problem &p, const mcsart_options &o)
+        : ctx(c), S(*c->driver), P(p), opt(o) {
+        V = nvox(P.g.nx, P.g.ny, P.g.nz);
+        NP = (int64_t)P.g.na * P.g.nb;
+        fp_bx = (int)div_up(P.g.na, 32);
+        fp_by = SUM == SUM_REF ? (int)div_up(P.g.nb, 8) : P.g.nb;
+        fp_blocks = fp_bx * fp_by;
+        groups = SUM == SUM_REF ? 8
+                 : opt.fp_groups > 0 ? std::min(opt.fp_groups, 8)
+                                     : fp_auto_groups(fp_blocks, std::max(P.g.nx, P.g.ny));
+        for (int v = 0; v < P.n_views; v++) views_img.push_back(v);
+        const int step = P.motion_model ? 1 : 10;  // AUMISART.cu:242 vs :72
+        for (int v = 1; v < P.n_views; v += step) views_mot.push_back(v);
+    }
+
+    Fields<ST> fields() const {
+        const ST *f = (const ST *)P.fields;
+        return Fields<ST>{f, f + V, f + 2 * V, f + 3 * V, f + 4 * V, f + 5 * V};
+    }
+    const ST *meas(int v) const { return (const ST *)P.proj + (int64_t)v * NP; }
+
+    int alloc() {
+        const size_t vs = V * sizeof(ST), vf = V * sizeof(float);
+        MC_TRY(S.img1.ensure(vs));
+        MC_TRY(S.img1T.ensure(vs));
+        MC_TRY(S.imgS.ensure(vs));
+        MC_TRY(S.imgST.ensure(vs));
+        MC_TRY(S.img0.ensure(vs));
+        MC_TRY(S.img0T.ensure(vs));
+        MC_TRY(S.ones.ensure(vs));
+        MC_TRY(S.onesT.ensure(vs));
+        MC_TRY(S.ratio.ensure(vf));
+        MC_TRY(S.imgT.ensure(vf));
+        MC_TRY(S.pairs.ensure(NP * sizeof(float2)));
+        if (INTERP == MCSART_INTERP_TEXTURE && P.motion_model) {
+            MC_TRY(S.tv_img.ensure(P.g.nx, P.g.ny, P.g.nz));
+            MC_TRY(S.tv_ratio.ensure(P.g.nx, P.g.ny, P.g.nz));
+        }
+        MC_TRY(S.norm_part.ensure((size_t)P.n_views * fp_blocks * sizeof(double2)));
+        MC_TRY(S.norm_tmp.ensure((size_t)P.n_views * sizeof(float)));
+        MC_TRY(S.views_image.ensure((size_t)P.n_views * sizeof(int)));
+        MC_TRY(S.views_motion.ensure((size_t)P.n_views * sizeof(int)));
+        MC_CHECK_CUDA(cudaMemcpyAsync(S.views_image.ptr, views_img.data(),
+                                      views_img.size() * sizeof(int), cudaMemcpyHostToDevice,
+                                      ctx->stream));
+        if (!views_mot.empty())
+            MC_CHECK_CUDA(cudaMemcpyAsync(S.views_motion.ptr, views_mot.data(),
+                                          views_mot.size() * sizeof(int),
+                                          cudaMemcpyHostToDevice, ctx->stream));
+        // the host vectors must stay valid until the copies ran
+        MC_CHECK_CUDA(cudaStreamSynchronize(ctx->stream));
+        return MCSART_OK;
+    }
+
+    template <int K, bool ONES, typename VT>
+    int launch_fp(const FPVolumes<VT, K> &vol, int v, int k, int mode) {
+        FPArgs<VT, K, ST> a{};
+        a.vol = vol;
+        a.g = P.g;
+        a.angle = P.angles[v];
+        a.angles = nullptr;
+        a.mode = mode;
+        a.meas = meas(v);
+        a.resid = (mode == FP_IMAGE && P.resid) ? P.resid + (int64_t)v * NP : nullptr;
+        a.bp_in = S.pairs.as<float2>();
+        a.norm_part = S.norm_part.as<double2>() + (int64_t)k * fp_blocks;
+        const dim3 grid(fp_bx, fp_by, 1), block(32, groups);
+        const size_t smem = SUM == SUM_REF ? 0 : (size_t)groups * (K + 1) * 32 * sizeof(float);
+        ctx->label = mode == FP_MOTION ? "fp_motion" : "fp_image";
+        MC_LAUNCH(ctx, (fp_kernel<K, ONES, SUM, VT, ST>), grid, block, smem, a);
+        return MCSART_OK;
+    }
+
+    int launch_bp(int v, int mode, float *out, float *outT, cudaSurfaceObject_t surf = 0) {
+        BPArgs b{};
+        b.outSurf = surf;
+        b.pair = S.pairs.as<float2>();
+        b.g = P.g;
+        b.angle = P.angles[v];
+        b.lambda = P.lambda;
+        b.out = out;
+        b.outT = outT;
+        const dim3 grid(div_up(P.g.nx, 32), div_up(P.g.ny, 32), P.g.nz), block(32, 8);
+        if (mode == BP_DIV) {
+            ctx->label = "bp_div";
+            MC_LAUNCH(ctx, (bp_kernel<2, BP_DIV>), grid, block, 0, b);
+        } else {
+            ctx->label = "bp_div_add";
+            MC_LAUNCH(ctx, (bp_kernel<2, BP_DIV_ADD>), grid, block, 0, b);
+        }
+        return MCSART_OK;
+    }
+
+    dim3 tile_grid() const { return dim3(div_up(P.g.nx, 32), div_up(P.g.ny, 32), P.g.nz); }
+
+    int finalize_norms(const int *views_dev, int n) {
+        if (n == 0) return MCSART_OK;
+        MC_LAUNCH(ctx, norm_finalize_kernel, div_up((int64_t)n * 32, 256), 256, 0,
+                  S.norm_tmp.as<float>(), S.norm_part.as<double2>(), fp_blocks, views_dev, n);
+        return MCSART_OK;
+    }
+
+    // AUMISART.cu:42-63
+    int enqueue_image_static() {
+        const Geom &g = P.g;
+        MC_CHECK_CUDA(cudaMemsetAsync(S.norm_tmp.ptr, 0, P.n_views * sizeof(float), ctx->stream));
+        MC_LAUNCH(ctx, (transpose_kernel<float, float>), tile_grid(), dim3(32, 8), 0,
+                  S.imgT.as<float>(), P.img, g.nx, g.ny);
+        FPVolumes<float, 1> vol{};
+        vol.std[0] = P.img;
+        vol.tr[0] = S.imgT.as<float>();
+        for (int k = 0; k < (int)views_img.size(); k++) {
+            const int v = views_img[k];
+            MC_TRY((launch_fp<1, true, float>(vol, v, k, FP_IMAGE)));
+            MC_TRY(launch_bp(v, BP_DIV_ADD, P.img, S.imgT.as<float>()));
+        }
+        return finalize_norms(S.views_image.as<int>(), (int)views_img.size());
+    }
+
+    // AUMISART.cu:184-233 with P = 1.  TEXTURE model: the volume and the
+    // normalised correction live in 3D arrays sampled by the texture unit; the
+    // backprojector and the update write them through surfaces, so the only
+    // copy is the volume's upload at the start of the pass.
+    int enqueue_image_mc() {
+        const Geom &g = P.g;
+        const Fields<ST> f = fields();
+        MC_CHECK_CUDA(cudaMemsetAsync(S.norm_tmp.ptr, 0, P.n_views * sizeof(float), ctx->stream));
+        const bool hw = INTERP == MCSART_INTERP_TEXTURE;
+        if (hw) MC_TRY(S.tv_img.upload(P.img, ctx->stream));
+        FPVolumes<ST, 1> vol{};
+        vol.std[0] = S.img1.as<ST>();
+        vol.tr[0] = S.img1T.as<ST>();
+        for (int k = 0; k < (int)views_img.size(); k++) {
+            const int v = views_img[k];
+            const float volume = P.volumes[v] - P.volumes[0];   // :193
+            const float flow = P.flows[v] - P.flows[0];
+            ctx->label = "warp_fwd";
+            if (hw) {
+                MC_LAUNCH(ctx, (warp_fwd_kernel<SrcTex, ST, ST>), tile_grid(), dim3(32, 8), 0,
+                          S.img1.as<ST>(), S.img1T.as<ST>(), SrcTex{S.tv_img.tex}, f, g.nx, g.ny,
+                          g.nz, volume, flow);
+            } else {
+                MC_LAUNCH(ctx, (warp_fwd_kernel<SrcLinear<float>, ST, ST>), tile_grid(),
+                          dim3(32, 8), 0, S.img1.as<ST>(), S.img1T.as<ST>(),
+                          SrcLinear<float>{P.img}, f, g.nx, g.ny, g.nz, volume, flow);
+            }
+            MC_TRY((launch_fp<1, true, ST>(vol, v, k, FP_IMAGE)));
+            if (hw)
+                MC_TRY(launch_bp(v, BP_DIV, nullptr, nullptr, S.tv_ratio.surf));
+            else
+                MC_TRY(launch_bp(v, BP_DIV, S.ratio.as<float>(), nullptr));
+            const float ivolume = P.volumes[0] - P.volumes[v];  // :222
+            const float iflow = P.flows[0] - P.flows[v];
+            ctx->label = "warp_back_add";
+            if (hw) {
+                MC_LAUNCH(ctx, (warp_back_add_kernel<SrcTex, ST>), stream_blocks(V), 256, 0,
+                          P.img, S.tv_img.surf, SrcTex{S.tv_ratio.tex}, f, g.nx, g.ny, g.nz,
+                          ivolume, iflow, P.lambda);
+            } else {
+                MC_LAUNCH(ctx, (warp_back_add_kernel<SrcLinear<float>, ST>), stream_blocks(V), 256,
+                          0, P.img, (cudaSurfaceObject_t)0,
+                          SrcLinear<float>{S.ratio.as<float>()}, f, g.nx, g.ny, g.nz, ivolume,
+                          iflow, P.lambda);
+            }
+        }
+        return finalize_norms(S.views_image.as<int>(), (int)views_img.size());
+    }
+
+    // AUMISART.cu:66-118 (step 10) / :236-288 (step 1)
+    int enqueue_motion() {
+        const Geom &g = P.g;
+        const Fields<ST> f = fields();
+        ST *fw = (ST *)P.fields;
+        MC_CHECK_CUDA(cudaMemsetAsync(S.norm_tmp.ptr, 0, P.n_views * sizeof(float), ctx->stream));
+        FPVolumes<ST, 3> vol{};
+        if (sizeof(ST) == sizeof(float)) {
+            vol.std[0] = (const ST *)P.img;
+        } else {
+            MC_LAUNCH(ctx, (cast_kernel<ST>), stream_blocks(V), 256, 0, S.imgS.as<ST>(),
+                      (const float *)P.img, V);
+            vol.std[0] = S.imgS.as<ST>();
+        }
+        MC_LAUNCH(ctx, (transpose_kernel<float, ST>), tile_grid(), dim3(32, 8), 0,
+                  S.imgST.as<ST>(), (const float *)P.img, g.nx, g.ny);
+        vol.tr[0] = S.imgST.as<ST>();
+        vol.std[1] = S.img0.as<ST>();
+        vol.tr[1] = S.img0T.as<ST>();
+        vol.std[2] = S.ones.as<ST>();
+        vol.tr[2] = S.onesT.as<ST>();
+        for (int k = 0; k < (int)views_mot.size(); k++) {
+            const int v = views_mot[k];
+            const float vd = P.volumes[v] - P.volumes[v - 1];  // :249-250
+            const float fd = P.flows[v] - P.flows[v - 1];
+            ctx->label = "motion_prep";
+            MC_LAUNCH(ctx, (motion_prep_kernel<ST, ST>), tile_grid(), dim3(32, 8), 0,
+                      S.img0.as<ST>(), S.img0T.as<ST>(), S.ones.as<ST>(), S.onesT.as<ST>(),
+                      (const float *)P.img, f, g.nx, g.ny, g.nz, vd, fd);
+            MC_TRY((launch_fp<3, false, ST>(vol, v, k, FP_MOTION)));
+            MC_TRY(launch_bp(v, BP_DIV, S.ratio.as<float>(), nullptr));
+            const float nvd = P.volumes[v - 1] - P.volumes[v];  // :272-277
+            const float nfd = P.flows[v - 1] - P.flows[v];
+            ctx->label = "field_update";
+            MC_LAUNCH(ctx, (field_update_kernel<ST>), tile_grid(), dim3(32, 8), 0, fw, fw + V,
+                      fw + 2 * V, fw + 3 * V, fw + 4 * V, fw + 5 * V,
+                      (const float *)S.ratio.as<float>(), (const float *)P.img, g.nx, g.ny, g.nz,
+                      nvd, nfd);
+        }
+        return finalize_norms(S.views_motion.as<int>(), (int)views_mot.size());
+    }
+
+    int enqueue(int kind) {
+        switch (kind) {
+            case PASS_IMAGE_STATIC: return enqueue_image_static();
+            case PASS_IMAGE_MC: return enqueue_image_mc();
+            default: return enqueue_motion();
+        }
+    }
+
+    std::vector<uint8_t> graph_key(int kind) const {
+        std::vector<uint8_t> k;
+        auto put = [&](const void *p, size_t n) {
+            const uint8_t *b = (const uint8_t *)p;
+            k.insert(k.end(), b, b + n);
+        };
+        const int hdr[7] = {kind, (int)sizeof(ST), INTERP, SUM, groups, (int)P.motion_model,
+                            (int)views_mot.size()};
+        put(hdr, sizeof(hdr));
+        put(views_img.data(), views_img.size() * sizeof(int));
+        put(views_mot.data(), views_mot.size() * sizeof(int));
+        put(&P.g, sizeof(Geom));
+        put(&P.n_views, sizeof(int));
+        put(&P.lambda, sizeof(float));
+        const void *ptrs[4] = {P.img, P.proj, P.fields, P.resid};
+        put(ptrs, sizeof(ptrs));
+        const void *bufs[6] = {S.img1.ptr, S.pairs.ptr, S.norm_part.ptr, S.ratio.ptr,
+                               (const void *)S.tv_img.arr, (const void *)S.tv_ratio.arr};
+        put(bufs, sizeof(bufs));
+        put(P.angles, P.n_views * sizeof(float));
+        put(P.volumes, P.n_views * sizeof(float));
+        put(P.flows, P.n_views * sizeof(float));
+        return k;
+    }
+
+    int run_pass(int kind) {
+        if (!opt.use_graph || ctx->profiling) return enqueue(kind);
+        PassGraph &pg = S.graphs[kind];
+        std::vector<uint8_t> key = graph_key(kind);
+        if (pg.exec == nullptr || pg.key != key) {
+            pg.release();
+            // Capture on the context's own stream: the caller's stream may be the
+            // legacy default stream, which cannot be captured.  Capturing runs
+            // nothing, so no ordering with the caller's stream is needed here.
+            cudaStream_t user = ctx->stream;
+            ctx->stream = ctx->own_stream;
+            cudaError_t eb = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
+            if (eb != cudaSuccess) {
+                ctx->stream = user;
+                MC_CHECK_CUDA(eb);
+            }
+            const long long before = ctx->launches;
+            const int rc = enqueue(kind);
+            cudaGraph_t graph = nullptr;
+            const cudaError_t ec = cudaStreamEndCapture(ctx->stream, &graph);
+            ctx->stream = user;
+            if (rc != MCSART_OK) {
+                if (graph) cudaGraphDestroy(graph);
+                return rc;
+            }
+            MC_CHECK_CUDA(ec);
+            const cudaError_t ei = cudaGraphInstantiate(&pg.exec, graph, 0);
+            cudaGraphDestroy(graph);
+            MC_CHECK_CUDA(ei);
+            pg.key = std::move(key);
+            pg.kernels = ctx->launches - before;
+            ctx->launches = before;
+        }
+        MC_CHECK_CUDA(cudaGraphLaunch(pg.exec, ctx->stream));
+        ctx->launches += pg.kernels;
+        return MCSART_OK;
+    }
+
+    int run(int n_iter, const int *op_iter, float *norm_out) {
+        MC_TRY(alloc());
+        for (int it = 0; it < n_iter; it++) {
+            int kind;
+            if (op_iter[it] == 1)
+                kind = P.motion_model ? PASS_IMAGE_MC : PASS_IMAGE_STATIC;
+            else
+                kind = PASS_MOTION;
+            MC_TRY(run_pass(kind));
+            if (norm_out)
+                MC_CHECK_CUDA(cudaMemcpyAsync(norm_out + (int64_t)it * P.n_views, S.norm_tmp.ptr,
+                                              P.n_views * sizeof(float), cudaMemcpyDeviceToDevice,
+                                              ctx->stream));
+        }
+        return MCSART_OK;
+    }
+};
+
+template <typename ST>
+int run_typed(mcsart_ctx *ctx, const Problem &P, int n_iter, const int *op_iter, float *norm_out,
+              const mcsart_options &opt) {
+#define MC_RUN(I, S) return Runner<ST, I, S>(ctx, P, opt).run(n_iter, op_iter, norm_out)
+    if (opt.interp == MCSART_INTERP_TEXTURE) {
+        if (opt.fp_sum == SUM_REF) MC_RUN(MCSART_INTERP_TEXTURE, SUM_REF);
+        if (opt.fp_sum == SUM_PLAIN) MC_RUN(MCSART_INTERP_TEXTURE, SUM_PLAIN);
+        MC_RUN(MCSART_INTERP_TEXTURE, SUM_KAHAN);
+    }
+    if (opt.fp_sum == SUM_REF) MC_RUN(MCSART_INTERP_EXACT, SUM_REF);
+    if (opt.fp_sum == SUM_PLAIN) MC_RUN(MCSART_INTERP_EXACT, SUM_PLAIN);
+    MC_RUN(MCSART_INTERP_EXACT, SUM_KAHAN);
+#undef MC_RUN
+}
+
+int run_driver(mcsart_ctx *ctx, const Problem &P, int n_iter, const int *op_iter, float *norm_out,
+               const mcsart_options &opt) {
+    if (!ctx->driver) ctx->driver.reset(new DriverState());
+    switch (opt.storage) {
+        case MCSART_F32: return run_typed<float>(ctx, P, n_iter, op_iter, norm_out, opt);
+        case MCSART_BF16: return run_typed<__nv_bfloat16>(ctx, P, n_iter, op_iter, norm_out, opt);
+        case MCSART_F16: return run_typed<__half>(ctx, P, n_iter, op_iter, norm_out, opt);
+        default: set_error("unknown storage type %d", opt.storage); return MCSART_ERR_INVALID_ARGUMENT;
+    }
+}
+
+int validate_options(const mcsart_options &o) {
+    MC_REQUIRE(o.storage >= MCSART_F32 && o.storage <= MCSART_F16, "unknown storage type %d",
+               o.storage);
+    MC_REQUIRE(o.interp == MCSART_INTERP_TEXTURE || o.interp == MCSART_INTERP_EXACT,
+               "unknown interpolation model %d", o.interp);
+    MC_REQUIRE(o.fp_groups >= 0 && o.fp_groups <= 8, "fp_groups must be in [0, 8]");
+    MC_REQUIRE(o.fp_sum >= SUM_REF && o.fp_sum <= SUM_KAHAN, "fp_sum must be 0, 1 or 2");
+    return MCSART_OK;
+}
+
+int validate_iter(int n_views, int n_iter, const int *op_iter, const float *angles,
+                  const float *volumes, const float *flows) {
+    MC_REQUIRE(n_views > 0, "n_views must be positive");
+    MC_REQUIRE(n_iter >= 0, "n_iter must be >= 0");
+    MC_REQUIRE(n_iter == 0 || op_iter, "op_iter must be non-NULL");
+    MC_REQUIRE(angles && volumes && flows, "angles, volumes and flows must be non-NULL");
+    return MCSART_OK;
+}
+
+}  // namespace mcsart
+
+using namespace mcsart;
+
+MC_EXPORT void mcsart_default_options(mcsart_options *opt) {
+    if (!opt) return;
+    opt->storage = MCSART_F32;
+    opt->interp = MCSART_INTERP_TEXTURE;
+    opt->use_graph = 1;
+    opt->fp_sum = SUM_REF;
+    opt->fp_groups = 0;
+}
+
+MC_EXPORT int mcsart_aumisart_device(mcsart_ctx *ctx, const mcsart_problem *prob, int n_iter,
+                                     const int *h_op_iter, const mcsart_options *opt_in) {
+    clear_error();
+    MC_TRY(validate_ctx(ctx));
+    MC_REQUIRE(prob, "problem is NULL");
+    mcsart_options opt;
+    if (opt_in) opt = *opt_in; else mcsart_default_options(&opt);
+    MC_TRY(validate_options(opt));
+    Geom g;
+    g.SO = prob->SO; g.SD = prob->SD; g.da = prob->da; g.ai = prob->ai; g.db = prob->db;
+    g.bi = prob->bi; g.na = prob->na; g.nb = prob->nb; g.nx = prob->nx; g.ny = prob->ny;
+    g.nz = prob->nz;
+    MC_TRY(validate_geom(g));
+    MC_TRY(validate_iter(prob->n_views, n_iter, h_op_iter, prob->h_angles, prob->h_volumes,
+                         prob->h_flows));
+    MC_REQUIRE(prob->d_img && prob->d_proj, "d_img and d_proj must be non-NULL");
+    if (!ctx->driver) ctx->driver.reset(new DriverState());
+    DriverState &S = *ctx->driver;
+    const int64_t V = nvox(g.nx, g.ny, g.nz);
+    const size_t es = opt.storage == MCSART_F32 ? 4 : 2;
+    Problem P;
+    P.g = g;
+    P.n_views = prob->n_views;
+    P.lambda = prob->lambda;
+    P.angles = prob->h_angles;
+    P.volumes = prob->h_volumes;
+    P.flows = prob->h_flows;
+    P.img = prob->d_img;
+    P.proj = prob->d_proj;
+    P.motion_model = prob->d_fields != nullptr;
+    P.resid = prob->d_resid;
+    if (P.motion_model) {
+        P.fields = prob->d_fields;
+    } else {  // overload 1: the DVF starts at zero (AUMISART.cu:25-30)
+        MC_TRY(S.zero_fields.ensure(6 * V * es));
+        MC_CHECK_CUDA(cudaMemsetAsync(S.zero_fields.ptr, 0, 6 * V * es, ctx->stream));
+        P.fields = S.zero_fields.ptr;
+    }
+    if (prob->d_norm)
+        MC_CHECK_CUDA(cudaMemsetAsync(prob->d_norm, 0, (size_t)n_iter * prob->n_views * sizeof(float),
+                                      ctx->stream));
+    MC_TRY(run_driver(ctx, P, n_iter, h_op_iter, prob->d_norm, opt));
+    return finish(ctx, "mcsart_aumisart_device");
+}
+
+MC_EXPORT int mcsart_aumisart(mcsart_ctx *ctx, float *h_outimg, float *h_outproj,
+                              float *h_outnorm, float *h_outalphax, const float *h_img,
+                              const float *h_proj, int nx, int ny, int nz, int na, int nb,
+                              int outIter, int n_views, int n_iter, const int *op_iter, float da,
+                              float db, float ai, float bi, float SO, float SD, float dx,
+                              float lambda, const float *volumes, const float *flows,
+                              const float *err_weights, const float *angles, const float *ax,
+                              const float *ay, const float *az, const float *bx,
+                              const float *by, const float *bz) {
+    clear_error();
+    (void)outIter; (void)dx; (void)err_weights;  // unused by the reference as well
+    MC_TRY(validate_ctx(ctx));
+    Geom g;
+    g.SO = SO; g.SD = SD; g.da = da; g.ai = ai; g.db = db; g.bi = bi;
+    g.na = na; g.nb = nb; g.nx = nx; g.ny = ny; g.nz = nz;
+    MC_TRY(validate_geom(g));
+    MC_TRY(validate_iter(n_views, n_iter, op_iter, angles, volumes, flows));
+    MC_REQUIRE(h_outimg && h_outproj && h_outnorm && h_outalphax && h_img && h_proj,
+               "image, projection and output pointers must be non-NULL");
+    const bool motion = ax != nullptr;
+    MC_REQUIRE(!motion || (ay && az && bx && by && bz),
+               "alpha_x given: all six DVF fields must be non-NULL");
+    if (!ctx->driver) ctx->driver.reset(new DriverState());
+    DriverState &S = *ctx->driver;
+    const int64_t V = nvox(nx, ny, nz), NP = (int64_t)na * nb;
+    const size_t vb = V * sizeof(float), pb = (size_t)n_views * NP * sizeof(float);
+    MC_TRY(S.h_img.ensure(vb));
+    MC_TRY(S.h_proj.ensure(pb));
+    MC_TRY(S.h_fields.ensure(6 * vb));
+    MC_TRY(S.h_resid.ensure(pb));
+    MC_TRY(S.h_norm.ensure((size_t)std::max(1, n_iter * n_views) * sizeof(float)));
+    cudaStream_t st = ctx->stream;
+    MC_CHECK_CUDA(cudaMemcpyAsync(S.h_img.ptr, h_img, vb, cudaMemcpyHostToDevice, st));
+    MC_CHECK_CUDA(cudaMemcpyAsync(S.h_proj.ptr, h_proj, pb, cudaMemcpyHostToDevice, st));
+    float *F = S.h_fields.as<float>();
+    if (motion) {
+        const float *src[6] = {ax, ay, az, bx, by, bz};
+        for (int c = 0; c < 6; c++)
+            MC_CHECK_CUDA(cudaMemcpyAsync(F + c * V, src[c], vb, cudaMemcpyHostToDevice, st));
+    } else {
+        MC_CHECK_CUDA(cudaMemsetAsync(F, 0, 6 * vb, st));
+    }
+    MC_CHECK_CUDA(cudaMemsetAsync(S.h_resid.ptr, 0, pb, st));
+    MC_CHECK_CUDA(cudaMemsetAsync(S.h_norm.ptr, 0, (size_t)n_iter * n_views * sizeof(float), st));
+    Problem P;
+    P.g = g;
+    P.n_views = n_views;
+    P.lambda = lambda;
+    P.angles = angles;
+    P.volumes = volumes;
+    P.flows = flows;
+    P.img = S.h_img.as<float>();
+    P.proj = S.h_proj.ptr;
+    P.fields = F;
+    P.motion_model = motion;
+    P.resid = S.h_resid.as<float>();
+    mcsart_options opt;
+    mcsart_default_options(&opt);
+    opt.interp = ctx->interp;
+    MC_TRY(run_driver(ctx, P, n_iter, op_iter, S.h_norm.as<float>(), opt));
+    MC_CHECK_CUDA(cudaMemcpyAsync(h_outimg, S.h_img.ptr, vb, cudaMemcpyDeviceToHost, st));
+    MC_CHECK_CUDA(cudaMemcpyAsync(h_outproj, S.h_resid.ptr, pb, cudaMemcpyDeviceToHost, st));
+    MC_CHECK_CUDA(cudaMemcpyAsync(h_outnorm, S.h_norm.ptr, (size_t)n_iter * n_views * sizeof(float),
+                                  cudaMemcpyDeviceToHost, st));
+    MC_CHECK_CUDA(cudaMemcpyAsync(h_outalphax, F, vb, cudaMemcpyDeviceToHost, st));
+    MC_CHECK_CUDA(cudaStreamSynchronize(st));
+    return MCSART_OK;
+}

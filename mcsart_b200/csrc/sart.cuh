@@ -1,0 +1,45 @@
+// Device-resident SART / motion driver state (the replacement of
+// host_AUMISART, src/AUMISART.cu:3-313).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <vector>
+
+#include "common.cuh"
+
+namespace mcsart {
+
+struct DevBuf {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    int ensure(size_t n);  // grow (contents undefined)
+    void release();
+    ~DevBuf() { release(); }
+    template <typename T> T *as() const { return (T *)ptr; }
+};
+
+struct PassGraph {
+    cudaGraphExec_t exec = nullptr;
+    std::vector<uint8_t> key;
+    long long kernels = 0;  // kernel nodes per replay
+    void release();
+    ~PassGraph() { release(); }
+};
+
+struct DriverState {
+    // working volumes of the passes
+    DevBuf img1, img1T, imgS, imgST, img0, img0T, ones, onesT, ratio, imgT;
+    DevBuf pairs, norm_part, norm_tmp, views_image, views_motion, zero_fields;
+    // staging for the host-pointer entry point
+    DevBuf h_img, h_proj, h_fields, h_resid, h_norm;
+    // 3D arrays sampled by the texture unit (INTERP_TEXTURE): the volume and
+    // the normalised correction of the image pass, and mcsart_deform's source
+    TexVol tv_img, tv_ratio, tv_deform;
+    std::map<int, PassGraph> graphs;  // keyed by pass kind
+    void invalidate_graphs() { graphs.clear(); }
+};
+
+}  // namespace mcsart

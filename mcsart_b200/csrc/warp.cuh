@@ -1,0 +1,148 @@
+// 5DCT deformation d(x,t) = a(t) v(x) + b(t) f(x) applied to a volume
+// (the reference's host_deform / kernel_forwardDVF / kernel_deformation,
+// src/cu_deform.cu:3-47,66-90, and the first-order host_deform2, :49-64,92-113).
+//
+// The displacement m = alpha*volume + beta*flow is formed in registers
+// (kernel_forwardDVF's three scratch volumes and their cudaMalloc/cudaFree per
+// call disappear).  The trilinear gather reads either a persistent 3D texture
+// (SrcTex: the texture unit's linear filtering, bit-identical to the
+// reference, whose filter weights are not plain products of 8-bit fractions)
+// or the linear volume in software with FP32 weights (SrcLinear, the EXACT
+// model).  The output keeps the reference's in-slice transposed indexing:
+// voxel (ix, iy, iz) of the sampling grid is written at iy + ix*ny + iz*nx*ny
+// and samples the source at texture coordinates (iy + my, ix + mx, iz + mz)
+// + 0.5 (:85-89).
+#pragma once
+
+#include "common.cuh"
+
+namespace mcsart {
+
+template <typename FT> struct Fields {
+    const FT *ax, *ay, *az, *bx, *by, *bz;
+};
+
+// Sample of `src` for output memory index id (any id in [0, nx*ny*nz)).
+template <typename SRC, typename FT>
+__device__ __forceinline__ float warp_sample(const SRC &src, const Fields<FT> &f, int64_t id,
+                                             int nx, int ny, int nz, float volume, float flow) {
+    const int64_t plane = (int64_t)nx * ny;
+    const int iz = (int)(id / plane);
+    const int64_t r = id - (int64_t)iz * plane;
+    const int ix = (int)(r / ny), iy = (int)(r - (int64_t)ix * ny);
+    // kernel_forwardDVF, cu_deform.cu:74-76
+    const float mx = ldv(f.ax, id) * volume + ldv(f.bx, id) * flow;
+    const float my = ldv(f.ay, id) * volume + ldv(f.by, id) * flow;
+    const float mz = ldv(f.az, id) * volume + ldv(f.bz, id) * flow;
+    // kernel_deformation, cu_deform.cu:86-89
+    const float xi = iy + 1.0f + my;
+    const float yi = ix + 1.0f + mx;
+    const float zi = iz + 1.0f + mz;
+    return src.fetch(xi - 0.5f, yi - 0.5f, zi - 0.5f, nx, ny, nz);
+}
+
+// Drop-in host_deform: out[id] = warp(src)[id] for all id.
+template <typename SRC>
+static __global__ void __launch_bounds__(256) deform_kernel(float *out, const SRC src,
+                                                            Fields<float> f, int nx, int ny,
+                                                            int nz, float volume, float flow) {
+    const int64_t n = nvox(nx, ny, nz);
+    for (int64_t id = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; id < n;
+         id += (int64_t)gridDim.x * blockDim.x)
+        out[id] = warp_sample(src, f, id, nx, ny, nz, volume, flow);
+}
+
+// Drop-in kernel_forwardDVF.
+static __global__ void __launch_bounds__(256) forward_dvf_kernel(float *mx, float *my, float *mz,
+                                                                 Fields<float> f, int64_t n,
+                                                                 float volume, float flow) {
+    for (int64_t id = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; id < n;
+         id += (int64_t)gridDim.x * blockDim.x) {
+        mx[id] = f.ax[id] * volume + f.bx[id] * flow;
+        my[id] = f.ay[id] * volume + f.by[id] * flow;
+        mz[id] = f.az[id] * volume + f.bz[id] * flow;
+    }
+}
+
+// Drop-in host_deform2 (first-order warp).  Neighbour reads that fall past
+// the end of the volume (the +nx neighbour of the last rows of the last slice
+// under the transposed index) read 0; the reference reads out of bounds there.
+static __global__ void __launch_bounds__(256) deform2_kernel(float *out, const float *in,
+                                                             Fields<float> f, int nx, int ny,
+                                                             int nz, float volume, float flow) {
+    const int64_t n = nvox(nx, ny, nz), plane = (int64_t)nx * ny;
+    for (int64_t id = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; id < n;
+         id += (int64_t)gridDim.x * blockDim.x) {
+        const int iz = (int)(id / plane);
+        const int64_t r = id - (int64_t)iz * plane;
+        const int ix = (int)(r / ny), iy = (int)(r - (int64_t)ix * ny);
+        const float mx = f.ax[id] * volume + f.bx[id] * flow;
+        const float my = f.ay[id] * volume + f.by[id] * flow;
+        const float mz = f.az[id] * volume + f.bz[id] * flow;
+        const float c = in[id];
+        auto at = [&](int64_t j) { return j < n ? in[j] : 0.0f; };
+        float dx, dy, dz;
+        if (ix == nx - 1) dx = 0; else dx = at(id + 1) - c;
+        if (iy == ny - 1) dy = 0; else dy = at(id + nx) - c;
+        if (iz == nz - 1) dz = 0; else dz = at(id + plane) - c;
+        out[id] = c + dy * mx + dx * my + dz * mz;  // cu_deform.cu:112
+    }
+}
+
+// SART image pass, forward warp of the current volume into the view's phase:
+// dst[id] = warp(src)[id] stored in VT, plus the y-fastest copy
+// dstT[iy + ix*ny] of the result (x-fastest reading) for the projector.
+// blockDim (32, 8); block covers a 32x32 (x, y) tile of slice blockIdx.z.
+template <typename SRC, typename FT, typename VT>
+static __global__ void __launch_bounds__(256) warp_fwd_kernel(VT *dst, VT *dstT, const SRC src,
+                                                              Fields<FT> f, int nx, int ny,
+                                                              int nz, float volume, float flow) {
+    __shared__ float tile[32][33];
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int x0 = blockIdx.x * 32, y0 = blockIdx.y * 32, iz = blockIdx.z;
+    const int64_t slice = (int64_t)iz * nx * ny;
+    const int xm = x0 + tx;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const int ly = ty + 8 * k, ym = y0 + ly;
+        float v = 0.0f;
+        if (xm < nx && ym < ny) {
+            const int64_t id = xm + (int64_t)ym * nx + slice;
+            v = warp_sample(src, f, id, nx, ny, nz, volume, flow);
+            dst[id] = cvt<VT>(v);
+        }
+        tile[ly][tx] = v;
+    }
+    __syncthreads();
+    const int ymT = y0 + tx;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const int lx = ty + 8 * k, xmT = x0 + lx;
+        if (xmT < nx && ymT < ny) dstT[ymT + (int64_t)xmT * ny + slice] = cvt<VT>(tile[tx][lx]);
+    }
+}
+
+// SART image pass, backward warp of the normalised correction and update:
+// img[id] += lambda * warp(src)[id]  (AUMISART.cu:222-223).  With a surface,
+// the updated voxel is also written to the 3D array the next forward warp
+// samples through the texture unit.
+template <typename SRC, typename FT>
+static __global__ void __launch_bounds__(256) warp_back_add_kernel(
+    float *img, cudaSurfaceObject_t img_surf, const SRC src, Fields<FT> f, int nx, int ny,
+    int nz, float volume, float flow, float lambda) {
+    const int64_t n = nvox(nx, ny, nz), plane = (int64_t)nx * ny;
+    for (int64_t id = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; id < n;
+         id += (int64_t)gridDim.x * blockDim.x) {
+        const float w = warp_sample(src, f, id, nx, ny, nz, volume, flow);
+        const float v = __fmaf_rn(w, lambda, img[id]);  // cu_add.cu:17
+        img[id] = v;
+        if (img_surf) {
+            const int z = (int)(id / plane);
+            const int64_t r = id - (int64_t)z * plane;
+            const int y = (int)(r / nx), x = (int)(r - (int64_t)y * nx);
+            surf3Dwrite(v, img_surf, x * (int)sizeof(float), y, z, cudaBoundaryModeZero);
+        }
+    }
+}
+
+}  // namespace mcsart
