@@ -48,6 +48,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the mixed-precision and fast-FP32 side measurements")
+    ap.add_argument("--profile-steps", type=int, default=0,
+                    help="only run this many untimed steps inside the NVTX range "
+                         "'mcsart_step' (for a profiler's launch list) and exit")
     return ap.parse_args()
 
 
@@ -200,7 +203,7 @@ def run_reference_arm(args, rank: int):
     threads = cpu_threads()
     O.set_num_threads(threads)
     proj = np.zeros((p.cfg.n_views, p.cfg.nb, p.cfg.na), np.float32)
-    views = args.cpu_views or 6
+    views = args.cpu_views or 32
     # only the views the sample touches need measured data
     for v in range(views + 1):
         vol = O.deform(p.truth, np.float32(p.volumes[v] - p.volumes[0]),
@@ -306,6 +309,18 @@ def main():
         return total, launches
 
     drop_in = m.default_options()  # FP32, texture-model warp, reference summation order
+    if args.profile_steps:
+        for _ in range(args.profile_steps):
+            torch.cuda.nvtx.range_push("mcsart_step")
+            step(drop_in, img, F)
+            torch.cuda.nvtx.range_pop()
+        torch.cuda.synchronize()
+        if rank == 0:
+            print(json.dumps({"profile_steps": args.profile_steps, "launches": ctx.launches}))
+        ctx.close()
+        if dist_on:
+            dist.destroy_process_group()
+        return
     clocks = ClockSampler(local)
     clocks.start()
     total, launches = timed(drop_in, args.steps, args.warmup, img, F)
@@ -399,7 +414,7 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = cpu_threads()
         h_proj_np = proj.cpu().numpy()
-        views = args.cpu_views or 8
+        views = args.cpu_views or 16
         dt, rate, views = cpu_sample(p, h_proj_np, views, threads)
         cpu = {"value": rate, "unit": "iterations/s", "cores": threads, "kind": "port",
                "sample": f"{views} views of the image pass + {views - 1} of the DVF-update "

@@ -34,9 +34,12 @@ __device__ __forceinline__ BPBox bp_box(int ix, int iy, int iz, float cphi, floa
     const float xc = (float)ix - g.nx / 2 + 0.5f;
     const float yc = (float)iy - g.ny / 2 + 0.5f;
     const float zc = (float)iz - g.nz / 2 + 0.5f;
-    // rotated voxel centre; the boundary points differ by +-0.5 from it
-    const float t = +xc * cphi + yc * sphi;
-    const float u = -xc * sphi + yc * cphi;
+    // rotated voxel centre; the boundary points differ by +-0.5 from it.  The
+    // products are fused explicitly in the order that reproduces the
+    // reference kernel bit for bit (":80-95" as compiled), so that the result
+    // does not depend on how the compiler contracts after unrolling.
+    const float t = __fmaf_rn(yc, sphi, __fmul_rn(xc, cphi));
+    const float u = __fmaf_rn(yc, cphi, __fmul_rn(-xc, sphi));
     const float tl = t - 0.5f, tr = t + 0.5f, ul = u - 0.5f, ur = u + 0.5f;
     const float rl = g.SD / (tl + g.SO);  // points ll and lr
     const float rr = g.SD / (tr + g.SO);  // points rr and rl

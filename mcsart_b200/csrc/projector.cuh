@@ -125,10 +125,49 @@ __device__ __forceinline__ void ray_slabs(const RayGeom &r, const FPVolumes<VT, 
         const float cz0 = __fadd_rn(__fmul_rn(r.rz0, dc), z_half);
         const float cz1 = __fadd_rn(__fmul_rn(r.rz1, dc), z_half);
         const float zi1 = fminf(cz0, cz1), zi2 = fmaxf(cz0, cz1);
-        const int u_lo = max(0, (int)floorf(ui1)), u_hi = min(r.nu - 1, (int)floorf(ui2));
-        const int z_lo = max(0, (int)floorf(zi1)), z_hi = min(g.nz - 1, (int)floorf(zi2));
-        if (u_lo > u_hi || z_lo > z_hi) continue;
+        const int U1 = (int)floorf(ui1), U2 = (int)floorf(ui2);
+        const int Z1 = (int)floorf(zi1), Z2 = (int)floorf(zi2);
         const float du = ui2 - ui1, dz = zi2 - zi1;
+        if (SUM == SUM_REF && U2 - U1 <= 1 && Z2 - Z1 <= 1) {
+            // The footprint fits a 2x2 voxel window (U1, U1+1) x (Z1, Z1+1): the
+            // reference's loops visit its in-volume members in this order, so
+            // evaluating the four candidates with predication gives the same
+            // sequence of fma's, without data-dependent trip counts.
+            const bool u0 = U1 >= 0 && U1 <= r.nu - 1;
+            const bool u1 = U1 + 1 <= U2 && U1 + 1 >= 0 && U1 + 1 <= r.nu - 1;
+            const bool z0 = Z1 >= 0 && Z1 <= g.nz - 1;
+            const bool z1 = Z1 + 1 <= Z2 && Z1 + 1 >= 0 && Z1 + 1 <= g.nz - 1;
+            const float fu0 = (float)U1, fu1 = (float)(U1 + 1);
+            const float fz0 = (float)Z1, fz1 = (float)(Z1 + 1);
+            const float wu0 = __fdiv_rn(fminf(fu0 + 1.0f, ui2) - fmaxf(fu0 + 0.0f, ui1), du);
+            const float wu1 = __fdiv_rn(fminf(fu1 + 1.0f, ui2) - fmaxf(fu1 + 0.0f, ui1), du);
+            const float wz0 = __fdiv_rn(fminf(fz0 + 1.0f, zi2) - fmaxf(fz0 + 0.0f, zi1), dz);
+            const float wz1 = __fdiv_rn(fminf(fz1 + 1.0f, zi2) - fmaxf(fz1 + 0.0f, zi1), dz);
+            // in-bounds addresses for every candidate (unused ones are not read)
+            const int cu0 = min(max(U1, 0), r.nu - 1), cu1 = min(max(U1 + 1, 0), r.nu - 1);
+            const int cz0 = min(max(Z1, 0), g.nz - 1), cz1 = min(max(Z1 + 1, 0), g.nz - 1);
+            const int64_t r0 = (int64_t)cu0 * su + (int64_t)d * sd;
+            const int64_t r1 = (int64_t)cu1 * su + (int64_t)d * sd;
+            const int64_t a00 = r0 + (int64_t)cz0 * sz, a01 = r0 + (int64_t)cz1 * sz;
+            const int64_t a10 = r1 + (int64_t)cz0 * sz, a11 = r1 + (int64_t)cz1 * sz;
+#pragma unroll
+            for (int k = 0; k < K; k++) {
+                if (u0 && z0) acc[k] = __fmaf_rn(ldv(base[k], a00) * wu0, wz0, acc[k]);
+                if (u0 && z1) acc[k] = __fmaf_rn(ldv(base[k], a01) * wu0, wz1, acc[k]);
+                if (u1 && z0) acc[k] = __fmaf_rn(ldv(base[k], a10) * wu1, wz0, acc[k]);
+                if (u1 && z1) acc[k] = __fmaf_rn(ldv(base[k], a11) * wu1, wz1, acc[k]);
+            }
+            if (ONES) {
+                if (u0 && z0) accw = __fmaf_rn(wu0, wz0, accw);
+                if (u0 && z1) accw = __fmaf_rn(wu0, wz1, accw);
+                if (u1 && z0) accw = __fmaf_rn(wu1, wz0, accw);
+                if (u1 && z1) accw = __fmaf_rn(wu1, wz1, accw);
+            }
+            continue;
+        }
+        const int u_lo = max(0, U1), u_hi = min(r.nu - 1, U2);
+        const int z_lo = max(0, Z1), z_hi = min(g.nz - 1, Z2);
+        if (u_lo > u_hi || z_lo > z_hi) continue;
         float ss[K], ssw = 0.0f;
 #pragma unroll
         for (int k = 0; k < K; k++) ss[k] = 0.0f;

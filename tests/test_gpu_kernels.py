@@ -64,7 +64,8 @@ def test_backprojection_matches_reference_and_oracle(ctx, torch_cuda, ref, oracl
         mine = _bp(ctx, torch_cuda, proj, a, g)
         r = ref.backprojection(proj, a, g)
         o = oracle.backprojection(proj, a, g)
-        assert rel_l2(mine, r) <= 1e-5, (a, rel_l2(mine, r))
+        # same arithmetic in the same order as the reference kernel: bit for bit
+        np.testing.assert_array_equal(mine, r)
         assert rel_l2(mine, o) <= 1e-4, (a, rel_l2(mine, o))
 
 
@@ -82,7 +83,7 @@ def test_deform_matches_reference(ctx, torch_cuda, ref, oracle, shape, vf):
     ctx.synchronize()
     mine = host(d_out)
     r = ref.deform(img, vol, flow, F)
-    assert rel_l2(mine, r) <= 1e-5, rel_l2(mine, r)
+    np.testing.assert_array_equal(mine, r)  # the texture unit, as in the reference
     if vf == (0.0, 0.0) and shape[1] == shape[2]:
         np.testing.assert_array_equal(mine, img)  # zero DVF on square slices: identity
 
