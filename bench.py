@@ -203,7 +203,7 @@ def run_reference_arm(args, rank: int):
     threads = cpu_threads()
     O.set_num_threads(threads)
     proj = np.zeros((p.cfg.n_views, p.cfg.nb, p.cfg.na), np.float32)
-    views = args.cpu_views or 32
+    views = args.cpu_views or 64
     # only the views the sample touches need measured data
     for v in range(views + 1):
         vol = O.deform(p.truth, np.float32(p.volumes[v] - p.volumes[0]),
@@ -232,6 +232,17 @@ def run_reference_arm(args, rank: int):
             "note": "the reference has no CPU implementation; this is the FP32 OpenMP "
                     "transcription of its kernels and host_AUMISART loop"}
     print(json.dumps(line), flush=True)
+
+
+def max_over_ranks(x: float, device: str = "cuda") -> float:
+    """The maximum of x over all ranks of the default process group (x if none)."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()):
+        return float(x)
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
 
 
 def config_dict(p, args) -> dict:
@@ -301,11 +312,7 @@ def main():
         launches = ctx.launches - l0
         if dist_on:
             dist.barrier()
-        total = sum(a.elapsed_time(b) for a, b in ev) / 1000.0
-        if dist_on:
-            t = torch.tensor([total], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            total = float(t.item())
+        total = max_over_ranks(sum(a.elapsed_time(b) for a, b in ev) / 1000.0)
         return total, launches
 
     drop_in = m.default_options()  # FP32, texture-model warp, reference summation order
@@ -370,11 +377,7 @@ def main():
     t0 = time.perf_counter()
     for _ in range(args.steps):
         e2e_step()
-    e2e_total = time.perf_counter() - t0
-    if dist_on:
-        t = torch.tensor([e2e_total], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_total = float(t.item())
+    e2e_total = max_over_ranks(time.perf_counter() - t0)
     e2e = {"value": args.steps / e2e_total * world, "unit": "iterations/s",
            "h2d_bytes_per_step": int(h_img.nbytes + h_proj.nbytes + 6 * h_img.nbytes),
            "d2h_bytes_per_step": int(o_img.nbytes + o_proj.nbytes + o_norm.nbytes + o_ax.nbytes),
@@ -407,14 +410,15 @@ def main():
                 st()
             e1.record(stream)
             torch.cuda.synchronize()
-            extras[name] = {"value": args.steps / (e0.elapsed_time(e1) / 1000.0) * world,
+            ext = max_over_ranks(e0.elapsed_time(e1) / 1000.0)
+            extras[name] = {"value": args.steps / ext * world,
                             "unit": "iterations/s"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = cpu_threads()
         h_proj_np = proj.cpu().numpy()
-        views = args.cpu_views or 16
+        views = args.cpu_views or 160
         dt, rate, views = cpu_sample(p, h_proj_np, views, threads)
         cpu = {"value": rate, "unit": "iterations/s", "cores": threads, "kind": "port",
                "sample": f"{views} views of the image pass + {views - 1} of the DVF-update "

@@ -308,7 +308,8 @@ template <typename ST, int INTERP, int SUM> struct Runner {
             const uint8_t *b = (const uint8_t *)p;
             k.insert(k.end(), b, b + n);
         };
-        const int hdr[7] = {kind, (int)sizeof(ST), INTERP, SUM, groups, (int)P.motion_model,
+        // the storage type itself, not its size: BF16 and F16 are both 2 bytes
+        const int hdr[7] = {kind, opt.storage, INTERP, SUM, groups, (int)P.motion_model,
                             (int)views_mot.size()};
         put(hdr, sizeof(hdr));
         put(views_img.data(), views_img.size() * sizeof(int));
@@ -318,8 +319,10 @@ template <typename ST, int INTERP, int SUM> struct Runner {
         put(&P.lambda, sizeof(float));
         const void *ptrs[4] = {P.img, P.proj, P.fields, P.resid};
         put(ptrs, sizeof(ptrs));
-        const void *bufs[6] = {S.img1.ptr, S.pairs.ptr, S.norm_part.ptr, S.ratio.ptr,
-                               (const void *)S.tv_img.arr, (const void *)S.tv_ratio.arr};
+        const void *bufs[14] = {S.img1.ptr, S.img1T.ptr, S.imgS.ptr, S.imgST.ptr, S.img0.ptr,
+                                S.img0T.ptr, S.ones.ptr, S.onesT.ptr, S.ratio.ptr, S.imgT.ptr,
+                                S.pairs.ptr, S.norm_part.ptr, (const void *)S.tv_img.arr,
+                                (const void *)S.tv_ratio.arr};
         put(bufs, sizeof(bufs));
         put(P.angles, P.n_views * sizeof(float));
         put(P.volumes, P.n_views * sizeof(float));

@@ -122,6 +122,37 @@ def test_device_api_graph_and_direct_agree(ctx, torch_cuda, oracle):
     np.testing.assert_array_equal(outs[0][2], host_out["alpha_x"])
 
 
+def test_graph_cache_tells_bf16_from_f16_on_the_same_buffers(ctx, torch_cuda, oracle):
+    """BF16 and F16 storage have the same element size: a pass graph captured
+    for one must not be replayed for the other when the buffers coincide."""
+    import mcsart_b200 as m
+    torch = torch_cuda
+    g, it, img0, proj, F = make_case(oracle, motion=True, seed=3, op_iter=(1, 1))
+    nproj, nf = proj.size, np.stack(F).size
+    raw_p = torch.empty(nproj * 2, dtype=torch.uint8, device="cuda")
+    raw_f = torch.empty(nf * 2, dtype=torch.uint8, device="cuda")
+    d_img = torch.empty(img0.shape, dtype=torch.float32, device="cuda")
+
+    def run(storage, use_graph):
+        dt = torch.bfloat16 if storage == m.BF16 else torch.float16
+        p, f = raw_p.view(dt).view(proj.shape), raw_f.view(dt).view((6,) + img0.shape)
+        p.copy_(dev(torch, proj))
+        f.copy_(dev(torch, np.stack(F)))
+        d_img.copy_(dev(torch, img0))
+        opt = m.default_options(storage=storage, interp=m.INTERP_EXACT, fp_sum=2,
+                                use_graph=use_graph)
+        ctx.aumisart_device(geo=g, n_views=it["n_views"], lambda_=1.0, angles=it["angles"],
+                            volumes=it["volumes"], flows=it["flows"], img=d_img, proj=p,
+                            fields=f, n_iter=it["n_iter"], op_iter=it["op_iter"], options=opt)
+        ctx.synchronize()
+        return host(d_img)
+
+    direct = {s: run(s, 0) for s in (m.BF16, m.F16)}
+    assert not np.array_equal(direct[m.BF16], direct[m.F16])
+    for s in (m.BF16, m.F16, m.BF16):
+        np.testing.assert_array_equal(run(s, 1), direct[s])
+
+
 @pytest.mark.parametrize("storage,tol", [(0, 2e-5), (1, 1e-2), (2, 2e-3)])
 def test_mixed_precision_error_vs_fp64_oracle(ctx, torch_cuda, oracle, storage, tol):
     """Motion-compensated SART (5 image passes, fixed DVF) with FP32/BF16/FP16
