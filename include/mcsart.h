@@ -193,6 +193,50 @@ typedef struct {
 int mcsart_aumisart_device(mcsart_ctx *ctx, const mcsart_problem *prob, int n_iter,
                            const int *h_op_iter, const mcsart_options *opt);
 
+/* ------------------------------------------ allocation-free projector */
+/* Largest volume, nx*ny*nz, that mcsart_projection_noalloc accepts: 2^22
+ * voxels (e.g. 256x256x64), i.e. 16 MiB of FP32 scratch per device. */
+#define MCSART_NOALLOC_MAX_VOXELS 4194304
+
+/* mcsart_projection without any allocation.  No counterpart in the reference:
+ * host_projection (src/cu_projection.cu:7) is the operation, this is an
+ * added way to call it.
+ *
+ * Who needs it.  mcsart_projection keeps a scratch copy of the volume in its
+ * context and allocates it (cudaMalloc) the first time a size is seen; the
+ * context itself allocates a stream and events.  Some callers cannot allow
+ * that: a MEX function or service whose device memory is owned by another
+ * pool (MATLAB's gpuArray memory, PyTorch's caching allocator), where a
+ * private cudaMalloc can fail for lack of free memory although the pool has
+ * room; and a reconstruction loop running beside other GPU work, where a
+ * cudaMalloc or cudaFree can stall work on other streams.  This entry point
+ * takes a stream instead of a context, keeps its scratch in a fixed device
+ * array that is part of the library, and calls no cudaMalloc, cudaFree or
+ * allocating library.
+ *
+ * Same arguments and results as mcsart_projection (bitwise), except:
+ * - stream: the CUDA stream (cudaStream_t) to run on; NULL = legacy default
+ *   stream.  The call returns once the work is enqueued; kernel faults
+ *   surface at the caller's next synchronisation;
+ * - nx*ny*nz above MCSART_NOALLOC_MAX_VOXELS is rejected with
+ *   MCSART_ERR_INVALID_ARGUMENT (use mcsart_projection for larger volumes);
+ * - set-up: the first call on each device, with that device current, looks
+ *   up the scratch's address (cudaGetSymbolAddress) and loads the kernels.
+ *   Make that first call before any stream capture and outside time-critical
+ *   code; later calls on that device do no set-up;
+ * - nothing has to start at zero: the scratch is written before it is read
+ *   and every cell of d_proj is written;
+ * - all calls on one device share the one scratch.  Calls in one stream are
+ *   ordered and safe; calls whose execution can overlap (different streams
+ *   or host threads with nothing ordering them) race on it and can return
+ *   wrong projections.
+ * The device reserves the 16 MiB array when it loads this part of the
+ * library: at the first call under lazy module loading (the CUDA 12
+ * default), at context creation under CUDA_MODULE_LOADING=EAGER. */
+int mcsart_projection_noalloc(void *stream, float *d_proj, const float *d_img, float angle,
+                              float SO, float SD, float da, int na, float ai, float db, int nb,
+                              float bi, int nx, int ny, int nz);
+
 #ifdef __cplusplus
 }
 #endif

@@ -13,9 +13,9 @@ reference's interface:
 """
 from ._lib import (BF16, ERR_CUDA, ERR_INVALID_ARGUMENT, ERR_NO_DEVICE, ERR_OUT_OF_MEMORY, F16,
                    F32, INTERP_EXACT, INTERP_TEXTURE, LIB_PATH, McsartError, Options)
-from .engine import Context, default_options
+from .engine import Context, default_options, projection_noalloc
 
 __version__ = "1.0.0"
-__all__ = ["Context", "McsartError", "Options", "default_options", "LIB_PATH", "F32", "BF16",
+__all__ = ["Context", "McsartError", "Options", "default_options", "projection_noalloc", "LIB_PATH", "F32", "BF16",
            "F16", "INTERP_TEXTURE", "INTERP_EXACT", "ERR_CUDA", "ERR_INVALID_ARGUMENT",
            "ERR_NO_DEVICE", "ERR_OUT_OF_MEMORY"]

@@ -58,6 +58,8 @@ _GEO = [_F, _F, _F, _F, _I, _F, _F, _I, _F, _I, _I, _I]  # angle, SO, SD, da, na
 # name -> argtypes (after the context argument); every function returns int
 SIGNATURES = {
     "mcsart_projection": [_P, _P] + _GEO,
+    # first argument is a cudaStream_t here, not a context
+    "mcsart_projection_noalloc": [_P, _P] + _GEO,
     "mcsart_backprojection": [_P, _P] + _GEO,
     "mcsart_deform": [_P, _P, _I, _I, _I, _F, _F] + [_P] * 6,
     "mcsart_deform2": [_P, _P, _I, _I, _I, _F, _F] + [_P] * 6,

@@ -18,8 +18,8 @@ from . import _lib
 from ._lib import (BF16, F16, F32, INTERP_EXACT, INTERP_TEXTURE, McsartError, Options,
                    Problem, check)
 
-__all__ = ["Context", "McsartError", "Options", "default_options", "F32", "BF16", "F16",
-           "INTERP_TEXTURE", "INTERP_EXACT"]
+__all__ = ["Context", "McsartError", "Options", "default_options", "projection_noalloc", "F32",
+           "BF16", "F16", "INTERP_TEXTURE", "INTERP_EXACT"]
 
 
 def _ptr(x, name="buffer", dtype_bytes=None):
@@ -41,6 +41,20 @@ def _ptr(x, name="buffer", dtype_bytes=None):
 
 def _hptr(a: np.ndarray) -> int:
     return a.ctypes.data
+
+
+def projection_noalloc(d_proj, d_img, angle, SO, SD, da, na, ai, db, nb, bi, nx, ny, nz,
+                       stream=None):
+    """mcsart_projection_noalloc: host_projection's operation (include/cu_projection.h:7)
+    without a context and without allocating; scratch in a fixed device array
+    of MCSART_NOALLOC_MAX_VOXELS voxels.  stream: an int cudaStream_t, a
+    torch.cuda.Stream, or None for the legacy default stream."""
+    if stream is not None and not isinstance(stream, int):
+        stream = stream.cuda_stream
+    L = _lib.load()
+    check(L.mcsart_projection_noalloc(stream, _ptr(d_proj, "d_proj", 4), _ptr(d_img, "d_img", 4),
+                                      angle, SO, SD, da, na, ai, db, nb, bi, nx, ny, nz),
+          "mcsart_projection_noalloc")
 
 
 def default_options(**kw) -> Options:
