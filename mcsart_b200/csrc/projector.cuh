@@ -39,31 +39,43 @@ struct RayGeom {
 };
 
 // src/cu_projection.cu:23-39,48-51,67-68,101-104,120-121 for ray (ia, ib).
+// Every operation is pinned with an explicit rounding intrinsic: which
+// products the compiler fuses into fma's otherwise depends on the surrounding
+// code.  The fused forms below are the ones whose results equal the
+// reference kernel's bit for bit; they were selected by running every
+// combination of candidate forms against the rebuilt reference on ~300k rays
+// (3 geometries, 30 angles, both driving axes): x2 and y2 fuse the product
+// with cos, the edge offsets (da/2)*sin, (da/2)*cos fuse into the edges, the
+// axial edges are z2 -+ db/2 after rounding z2, the source offset is
+// subtracted unfused.
 __device__ __forceinline__ RayGeom ray_geom(float cphi, float sphi, int ia, int ib,
                                             const Geom &g) {
-    const float x1 = -g.SO * cphi, y1 = -g.SO * sphi, z1 = 0.0f;
-    const float x20 = g.SD - g.SO;
-    const float y20 = (ia + g.ai) * g.da;
-    const float x2 = x20 * cphi - y20 * sphi;
-    const float y2 = x20 * sphi + y20 * cphi;
-    const float z2 = (ib + g.bi) * g.db;
-    const float x21 = x2 - x1, y21 = y2 - y1, z21 = z2 - z1;
+    const float x1 = -__fmul_rn(g.SO, cphi), y1 = -__fmul_rn(g.SO, sphi);
+    const float x20 = __fsub_rn(g.SD, g.SO);
+    const float y20 = __fmul_rn(__fadd_rn((float)ia, g.ai), g.da);
+    const float x2 = __fmaf_rn(x20, cphi, -__fmul_rn(y20, sphi));
+    const float y2 = __fmaf_rn(y20, cphi, __fmul_rn(x20, sphi));
+    const float z2 = __fmul_rn(__fadd_rn((float)ib, g.bi), g.db);  // z21 = z2 - z1, z1 = 0
+    const float x21 = __fsub_rn(x2, x1), y21 = __fsub_rn(y2, y1);
     RayGeom r;
     r.xdrive = fabsf(x21) > fabsf(y21);
-    const float xl = x21 - g.da / 2 * sphi, xr = x21 + g.da / 2 * sphi;
-    const float yl = y21 - g.da / 2 * cphi, yr = y21 + g.da / 2 * cphi;
-    const float zl = z21 - g.db / 2, zr = z21 + g.db / 2;
+    const float hda = __fdiv_rn(g.da, 2.0f), hdb = __fdiv_rn(g.db, 2.0f);
+    const float xl = __fmaf_rn(-hda, sphi, x21), xr = __fmaf_rn(hda, sphi, x21);
+    const float yl = __fmaf_rn(-hda, cphi, y21), yr = __fmaf_rn(hda, cphi, y21);
+    const float zl = __fsub_rn(z2, hdb), zr = __fadd_rn(z2, hdb);
     if (r.xdrive) {
-        r.r0 = yl / xl; r.r1 = yl / xr; r.r2 = yr / xl; r.r3 = yr / xr;
-        r.rz0 = zl / x21; r.rz1 = zr / x21;
+        r.r0 = __fdiv_rn(yl, xl); r.r1 = __fdiv_rn(yl, xr);
+        r.r2 = __fdiv_rn(yr, xl); r.r3 = __fdiv_rn(yr, xr);
+        r.rz0 = __fdiv_rn(zl, x21); r.rz1 = __fdiv_rn(zr, x21);
         r.u_off = y1; r.u_half = (float)(g.ny / 2);
-        r.d_half = (float)g.nx / 2; r.src_d = x1;
+        r.d_half = __fdiv_rn((float)g.nx, 2.0f); r.src_d = x1;
         r.nd = g.nx; r.nu = g.ny;
     } else {
-        r.r0 = xl / yl; r.r1 = xl / yr; r.r2 = xr / yl; r.r3 = xr / yr;
-        r.rz0 = zl / y21; r.rz1 = zr / y21;
+        r.r0 = __fdiv_rn(xl, yl); r.r1 = __fdiv_rn(xl, yr);
+        r.r2 = __fdiv_rn(xr, yl); r.r3 = __fdiv_rn(xr, yr);
+        r.rz0 = __fdiv_rn(zl, y21); r.rz1 = __fdiv_rn(zr, y21);
         r.u_off = x1; r.u_half = (float)(g.nx / 2);
-        r.d_half = (float)g.ny / 2; r.src_d = y1;
+        r.d_half = __fdiv_rn((float)g.ny, 2.0f); r.src_d = y1;
         r.nd = g.ny; r.nu = g.nx;
     }
     return r;
@@ -127,7 +139,7 @@ __device__ __forceinline__ void ray_slabs(const RayGeom &r, const FPVolumes<VT, 
         const float zi1 = fminf(cz0, cz1), zi2 = fmaxf(cz0, cz1);
         const int U1 = (int)floorf(ui1), U2 = (int)floorf(ui2);
         const int Z1 = (int)floorf(zi1), Z2 = (int)floorf(zi2);
-        const float du = ui2 - ui1, dz = zi2 - zi1;
+        const float du = __fsub_rn(ui2, ui1), dz = __fsub_rn(zi2, zi1);
         if (SUM == SUM_REF && U2 - U1 <= 1 && Z2 - Z1 <= 1) {
             // The footprint fits a 2x2 voxel window (U1, U1+1) x (Z1, Z1+1): the
             // reference's loops visit its in-volume members in this order, so
@@ -139,10 +151,10 @@ __device__ __forceinline__ void ray_slabs(const RayGeom &r, const FPVolumes<VT, 
             const bool z1 = Z1 + 1 <= Z2 && Z1 + 1 >= 0 && Z1 + 1 <= g.nz - 1;
             const float fu0 = (float)U1, fu1 = (float)(U1 + 1);
             const float fz0 = (float)Z1, fz1 = (float)(Z1 + 1);
-            const float wu0 = __fdiv_rn(fminf(fu0 + 1.0f, ui2) - fmaxf(fu0 + 0.0f, ui1), du);
-            const float wu1 = __fdiv_rn(fminf(fu1 + 1.0f, ui2) - fmaxf(fu1 + 0.0f, ui1), du);
-            const float wz0 = __fdiv_rn(fminf(fz0 + 1.0f, zi2) - fmaxf(fz0 + 0.0f, zi1), dz);
-            const float wz1 = __fdiv_rn(fminf(fz1 + 1.0f, zi2) - fmaxf(fz1 + 0.0f, zi1), dz);
+            const float wu0 = __fdiv_rn(__fsub_rn(fminf(__fadd_rn(fu0, 1.0f), ui2), fmaxf(fu0, ui1)), du);
+            const float wu1 = __fdiv_rn(__fsub_rn(fminf(__fadd_rn(fu1, 1.0f), ui2), fmaxf(fu1, ui1)), du);
+            const float wz0 = __fdiv_rn(__fsub_rn(fminf(__fadd_rn(fz0, 1.0f), zi2), fmaxf(fz0, zi1)), dz);
+            const float wz1 = __fdiv_rn(__fsub_rn(fminf(__fadd_rn(fz1, 1.0f), zi2), fmaxf(fz1, zi1)), dz);
             // in-bounds addresses for every candidate (unused ones are not read)
             const int cu0 = min(max(U1, 0), r.nu - 1), cu1 = min(max(U1 + 1, 0), r.nu - 1);
             const int cz0 = min(max(Z1, 0), g.nz - 1), cz1 = min(max(Z1 + 1, 0), g.nz - 1);
@@ -152,10 +164,10 @@ __device__ __forceinline__ void ray_slabs(const RayGeom &r, const FPVolumes<VT, 
             const int64_t a10 = r1 + (int64_t)cz0 * sz, a11 = r1 + (int64_t)cz1 * sz;
 #pragma unroll
             for (int k = 0; k < K; k++) {
-                if (u0 && z0) acc[k] = __fmaf_rn(ldv(base[k], a00) * wu0, wz0, acc[k]);
-                if (u0 && z1) acc[k] = __fmaf_rn(ldv(base[k], a01) * wu0, wz1, acc[k]);
-                if (u1 && z0) acc[k] = __fmaf_rn(ldv(base[k], a10) * wu1, wz0, acc[k]);
-                if (u1 && z1) acc[k] = __fmaf_rn(ldv(base[k], a11) * wu1, wz1, acc[k]);
+                if (u0 && z0) acc[k] = __fmaf_rn(__fmul_rn(ldv(base[k], a00), wu0), wz0, acc[k]);
+                if (u0 && z1) acc[k] = __fmaf_rn(__fmul_rn(ldv(base[k], a01), wu0), wz1, acc[k]);
+                if (u1 && z0) acc[k] = __fmaf_rn(__fmul_rn(ldv(base[k], a10), wu1), wz0, acc[k]);
+                if (u1 && z1) acc[k] = __fmaf_rn(__fmul_rn(ldv(base[k], a11), wu1), wz1, acc[k]);
             }
             if (ONES) {
                 if (u0 && z0) accw = __fmaf_rn(wu0, wz0, accw);
@@ -173,20 +185,20 @@ __device__ __forceinline__ void ray_slabs(const RayGeom &r, const FPVolumes<VT, 
         for (int k = 0; k < K; k++) ss[k] = 0.0f;
         for (int u = u_lo; u <= u_hi; u++) {
             // :83 / :136
-            const float wu = __fdiv_rn(fminf(u + 1.0f, ui2) - fmaxf(u + 0.0f, ui1), du);
+            const float wu = __fdiv_rn(__fsub_rn(fminf(__fadd_rn((float)u, 1.0f), ui2), fmaxf((float)u, ui1)), du);
             const int64_t row = (int64_t)u * su + (int64_t)d * sd;
             for (int z = z_lo; z <= z_hi; z++) {
                 // :86 / :139
-                const float wz = __fdiv_rn(fminf(z + 1.0f, zi2) - fmaxf(z + 0.0f, zi1), dz);
+                const float wz = __fdiv_rn(__fsub_rn(fminf(__fadd_rn((float)z, 1.0f), zi2), fmaxf((float)z, zi1)), dz);
                 const int64_t a = row + (int64_t)z * sz;
                 if (SUM == SUM_REF) {
 #pragma unroll
                     for (int k = 0; k < K; k++)
-                        acc[k] = __fmaf_rn(ldv(base[k], a) * wu, wz, acc[k]);  // :87 / :140
+                        acc[k] = __fmaf_rn(__fmul_rn(ldv(base[k], a), wu), wz, acc[k]);  // :87 / :140
                     if (ONES) accw = __fmaf_rn(wu, wz, accw);
                 } else {
 #pragma unroll
-                    for (int k = 0; k < K; k++) ss[k] = __fmaf_rn(ldv(base[k], a) * wu, wz, ss[k]);
+                    for (int k = 0; k < K; k++) ss[k] = __fmaf_rn(__fmul_rn(ldv(base[k], a), wu), wz, ss[k]);
                     if (ONES) ssw = __fmaf_rn(wu, wz, ssw);
                 }
             }

@@ -2,7 +2,9 @@
 
 Parity bar: the FP32 drop-in must match the reference's own host_AUMISART,
 rebuilt from its sources and run on the same GPU and inputs, to 1e-4 relative
-L2 on the volume after 5 iterations; the same against the FP64 oracle.
+L2 on the volume after 5 iterations; the same against the FP64 oracle.  The
+engine meets it with zero difference: volume, alpha_x and residuals are bit
+for bit the reference's, after image and DVF passes.
 """
 import numpy as np
 import pytest
@@ -47,37 +49,38 @@ def run_engine(ctx, g, it, img0, proj, F):
 
 
 def test_static_sart_matches_reference_after_5_iterations(ctx, oracle):
-    """host_AUMISART overload 1 (static SART), 5 image passes: the volume
-    matches the reference's own loop, rebuilt from its sources, to 1e-4."""
+    """host_AUMISART overload 1 (static SART), 5 image passes, against the
+    reference's own loop rebuilt from its sources: the stated bar is 1e-4
+    relative L2 on the volume; volume and residuals agree bit for bit.  The
+    norm list (cublasSnrm2 in the reference, a fixed-order double sum here)
+    agrees to 1e-6."""
     from oracle import ref_runner
     g, it, img0, proj, F = make_case(oracle, motion=False, op_iter=(1, 1, 1, 1, 1))
     mine = run_engine(ctx, g, it, img0, proj, F)
     r = ref_runner.aumisart(img0, proj, g, it, F)
     assert rel_l2(mine["img"], r["img"]) <= 1e-4, rel_l2(mine["img"], r["img"])
-    assert rel_l2(mine["norm"], r["norm"]) <= 1e-4
-    assert rel_l2(mine["resid"], r["resid"]) <= 1e-4
+    np.testing.assert_array_equal(mine["img"], r["img"])
+    np.testing.assert_array_equal(mine["resid"], r["resid"])
+    assert rel_l2(mine["norm"], r["norm"]) <= 1e-6
 
 
-@pytest.mark.parametrize("op", [(1,), (1, 0), (1, 0, 1, 0, 1)])
-def test_motion_sart_matches_reference(ctx, oracle, op):
-    """host_AUMISART overload 2.  The image pass matches the reference to the
-    projector's rounding level.  The reference's DVF pass divides by
-    BP(FP(initial2(...))), a signed normaliser that crosses zero
-    (AUMISART.cu:267-270), so last-bit differences of the projector are
-    amplified: after one DVF pass alpha_x agrees to ~1e-3 and the volume after
-    five passes to ~1e-2 (an FP32 and an FP64 run of the same algorithm differ
-    by ~8% there)."""
+@pytest.mark.parametrize("seed", [0, 1])
+@pytest.mark.parametrize("op", [(1,), (1, 0), (1, 0, 1), (1, 0, 1, 0, 1)])
+def test_motion_sart_matches_reference(ctx, oracle, op, seed):
+    """host_AUMISART overload 2 against the rebuilt reference.  Its DVF pass
+    divides by BP(FP(initial2(...))), a signed normaliser that crosses zero
+    (AUMISART.cu:267-270), so any last-bit difference of a kernel grows by
+    orders of magnitude within a few passes; the engine reproduces every
+    kernel of the loop bit for bit, so volume, alpha_x and residuals agree
+    exactly after image and DVF passes alike."""
     from oracle import ref_runner
-    g, it, img0, proj, F = make_case(oracle, motion=True, op_iter=op)
+    g, it, img0, proj, F = make_case(oracle, motion=True, op_iter=op, seed=seed)
     mine = run_engine(ctx, g, it, img0, proj, F)
     r = ref_runner.aumisart(img0, proj, g, it, F)
-    tol = {1: 1e-6, 2: 1e-6, 5: 2e-2}[len(op)]
-    assert rel_l2(mine["img"], r["img"]) <= tol, rel_l2(mine["img"], r["img"])
-    if 0 in op:
-        assert rel_l2(mine["alpha_x"], r["alpha_x"]) <= (5e-3 if len(op) == 2 else 5e-2)
-    if len(op) == 1:
-        assert rel_l2(mine["norm"], r["norm"]) <= 1e-6
-        assert rel_l2(mine["resid"], r["resid"]) <= 1e-5
+    np.testing.assert_array_equal(mine["img"], r["img"])
+    np.testing.assert_array_equal(mine["alpha_x"], r["alpha_x"])
+    np.testing.assert_array_equal(mine["resid"], r["resid"])
+    assert rel_l2(mine["norm"], r["norm"]) <= 1e-6
 
 
 def test_static_sart_matches_oracle(ctx, oracle):
