@@ -47,8 +47,8 @@ int launch_fp_plain(mcsart_ctx *ctx, float *d_proj, const float *d_img, const fl
     a.mode = FP_PLAIN;
     a.out = d_proj;
     // the reference's summation order: bitwise the reference kernel's output
-    const dim3 grid(div_up(g.na, 32), div_up(g.nb, 8), n_views), block(32, 8);
-    MC_LAUNCH(ctx, (fp_kernel<K, false, SUM_REF, float>), grid, block, 0, a);
+    const dim3 grid(div_up(g.na, FPC_COLS), div_up(g.nb, FPC_ROWS), n_views);
+    MC_LAUNCH(ctx, (fp_ref_kernel<K, false, float>), grid, dim3(FPC_THREADS), 0, a);
     return MCSART_OK;
 }
 
@@ -130,7 +130,7 @@ MC_EXPORT int mcsart_backprojection(mcsart_ctx *ctx, float *d_img, const float *
     a.g = g;
     a.angle = angle;
     a.out = d_img;
-    const dim3 grid(div_up(nx, 32), div_up(ny, 32), nz), block(32, 8);
+    const dim3 grid(div_up(nx, 32), div_up(ny, BP_ROWS), div_up(nz, BP_NZ)), block(32, BP_ROWS);
     MC_LAUNCH(ctx, (bp_kernel<1, BP_PLAIN>), grid, block, 0, a);
     return finish(ctx, "mcsart_backprojection");
 }

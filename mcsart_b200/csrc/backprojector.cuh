@@ -10,10 +10,10 @@
 // fetch happens at texel centres (:167) and so returns the texel itself, which
 // removes the per-call cudaMalloc3DArray + copy (:10-37).
 //
-// Restructured for the hardware: one thread per voxel (no atomics, so runs are
-// bitwise reproducible), 32x32 voxel tiles per block for coalesced stores and
-// a shared-memory transpose when the y-fastest copy of the volume must be kept
-// current; two projections (SART residual and ones-projection, packed as
+// Restructured for the hardware: one thread per column of BP_NZ voxels (no
+// atomics, so runs are bitwise reproducible), 32-wide rows of voxels per warp
+// for coalesced stores and a shared-memory transpose when the y-fastest copy
+// of the volume must be kept current; two projections (SART residual and ones-projection, packed as
 // float2) are gathered with one set of weights and the SART division
 // (src/cu_division.cu:20-24) and update (src/cu_add.cu:17) run in the epilogue.
 #pragma once
@@ -24,16 +24,17 @@ namespace mcsart {
 
 enum BPMode { BP_PLAIN = 0, BP_DIV = 1, BP_DIV_ADD = 2 };
 
-struct BPBox {
-    float amin, amax, bmin, bmax;
+// In-plane part of the footprint of voxel column (ix, iy): the same for every
+// z (src/cu_backprojection.cu:66-67,80-122,135-136).
+struct BPColumn {
+    float amin, amax;  // detector column box, index units
+    float rl, rr, r0;  // magnifications SD/(x+SO) at the three distances
 };
 
-// src/cu_backprojection.cu:66-138 for voxel (ix, iy, iz).
-__device__ __forceinline__ BPBox bp_box(int ix, int iy, int iz, float cphi, float sphi,
-                                        const Geom &g) {
+__device__ __forceinline__ BPColumn bp_column(int ix, int iy, float cphi, float sphi,
+                                              const Geom &g) {
     const float xc = (float)ix - g.nx / 2 + 0.5f;
     const float yc = (float)iy - g.ny / 2 + 0.5f;
-    const float zc = (float)iz - g.nz / 2 + 0.5f;
     // rotated voxel centre; the boundary points differ by +-0.5 from it.  The
     // products are fused explicitly in the order that reproduces the
     // reference kernel bit for bit (":80-95" as compiled), so that the result
@@ -41,46 +42,27 @@ __device__ __forceinline__ BPBox bp_box(int ix, int iy, int iz, float cphi, floa
     const float t = __fmaf_rn(yc, sphi, __fmul_rn(xc, cphi));
     const float u = __fmaf_rn(yc, cphi, __fmul_rn(-xc, sphi));
     const float tl = t - 0.5f, tr = t + 0.5f, ul = u - 0.5f, ur = u + 0.5f;
-    const float rl = g.SD / (tl + g.SO);  // points ll and lr
-    const float rr = g.SD / (tr + g.SO);  // points rr and rl
-    const float r0 = g.SD / (t + g.SO);   // top and bottom
-    const float all = rl * ul, alr = rl * ur, arr = rr * ur, arl = rr * ul, at = r0 * u;
-    const float bl = rl * zc, br = rr * zc, bt = r0 * (zc + 0.5f), bb = r0 * (zc - 0.5f);
-    float amax = fmaxf(fmaxf(fmaxf(all, arr), fmaxf(alr, arl)), at);
-    float amin = fminf(fminf(fminf(all, arr), fminf(alr, arl)), at);
-    float bmax = fmaxf(fmaxf(fmaxf(bl, br), fmaxf(bl, br)), fmaxf(bt, bb));
-    float bmin = fminf(fminf(fminf(bl, br), fminf(bl, br)), fminf(bt, bb));
-    BPBox box;
-    box.amax = amax / g.da - g.ai + 0.5f;
-    box.amin = amin / g.da - g.ai + 0.5f;
-    box.bmax = bmax / g.db - g.bi + 0.5f;
-    box.bmin = bmin / g.db - g.bi + 0.5f;
-    return box;
+    BPColumn c;
+    c.rl = g.SD / (tl + g.SO);  // points ll and lr
+    c.rr = g.SD / (tr + g.SO);  // points rr and rl
+    c.r0 = g.SD / (t + g.SO);   // top and bottom
+    const float all = c.rl * ul, alr = c.rl * ur, arr = c.rr * ur, arl = c.rr * ul, at = c.r0 * u;
+    const float amax = fmaxf(fmaxf(fmaxf(all, arr), fmaxf(alr, arl)), at);
+    const float amin = fminf(fminf(fminf(all, arr), fminf(alr, arl)), at);
+    c.amax = amax / g.da - g.ai + 0.5f;
+    c.amin = amin / g.da - g.ai + 0.5f;
+    return c;
 }
 
-// Overlap-weighted gather of K projections over the box (:150-168).
-template <int K>
-__device__ __forceinline__ void bp_gather(const BPBox &bx, const float *p1, const float2 *p2,
-                                          const Geom &g, float *acc) {
-    const float alim = ((float)g.na < bx.amax) ? (float)g.na : bx.amax;  // MIN(na, a_max)
-    const float blim = ((float)g.nb < bx.bmax) ? (float)g.nb : bx.bmax;
-    const int ia0 = max(0, (int)floorf(fmaxf(bx.amin, -1.0f)));
-    const int ib0 = max(0, (int)floorf(fmaxf(bx.bmin, -1.0f)));
-    for (int ia = ia0; (float)ia < alim; ia++) {
-        const float wa = fminf(ia + 1.0f, bx.amax) - fmaxf(ia + 0.0f, bx.amin);
-        for (int ib = ib0; (float)ib < blim; ib++) {
-            const float wb = fminf(ib + 1.0f, bx.bmax) - fmaxf(ib + 0.0f, bx.bmin);
-            const float w = wa * wb;
-            const int64_t pix = ia + (int64_t)ib * g.na;
-            if (K == 1) {
-                acc[0] = __fmaf_rn(w, __ldg(p1 + pix), acc[0]);
-            } else {
-                const float2 v = __ldg(p2 + pix);
-                acc[0] = __fmaf_rn(w, v.x, acc[0]);
-                acc[1] = __fmaf_rn(w, v.y, acc[1]);
-            }
-        }
-    }
+// Axial part for slice iz (:68,96-97,115-122,137-138): detector row box.
+__device__ __forceinline__ void bp_rows(const BPColumn &c, int iz, const Geom &g, float &bmin,
+                                        float &bmax) {
+    const float zc = (float)iz - g.nz / 2 + 0.5f;
+    const float bl = c.rl * zc, br = c.rr * zc, bt = c.r0 * (zc + 0.5f), bb = c.r0 * (zc - 0.5f);
+    const float hi = fmaxf(fmaxf(fmaxf(bl, br), fmaxf(bl, br)), fmaxf(bt, bb));
+    const float lo = fminf(fminf(fminf(bl, br), fminf(bl, br)), fminf(bt, bb));
+    bmax = hi / g.db - g.bi + 0.5f;
+    bmin = lo / g.db - g.bi + 0.5f;
 }
 
 struct BPArgs {
@@ -95,30 +77,122 @@ struct BPArgs {
     cudaSurfaceObject_t outSurf;  // BP_DIV: 3D array receiving the ratio (0 = none)
 };
 
-// blockDim = (32, 8); each block covers a 32x32 (x, y) tile of slice blockIdx.z.
+// Voxel columns per block: 32 (x) by BP_ROWS (y), BP_NZ slices per thread.
+#ifndef MCSART_BP_NZ
+#define MCSART_BP_NZ 2
+#endif
+#ifndef MCSART_BP_MINBLOCKS
+#define MCSART_BP_MINBLOCKS 1
+#endif
+constexpr int BP_ROWS = 8;
+constexpr int BP_NZ = MCSART_BP_NZ;
+// Row weights kept in registers per slice; footprints taller than this many
+// detector rows take the general loop.
+constexpr int BP_WB = 4;
+
+// blockDim = (32, BP_ROWS); each thread backprojects the BP_NZ voxels
+// (ix, iy, z0 .. z0 + BP_NZ - 1), z0 = blockIdx.z * BP_NZ.  Per voxel the
+// terms are accumulated in the reference's order (detector column outer,
+// row inner, acc = fma(wa*wb, p, acc), :150-168); the column box and the
+// column weights wa are shared by the voxels of a thread, the row weights wb
+// are computed once per voxel instead of once per (column, row).
 template <int K, int MODE>
-__global__ void __launch_bounds__(256) bp_kernel(const BPArgs p) {
-    __shared__ float tile[32][33];
+__global__ void __launch_bounds__(256, MCSART_BP_MINBLOCKS) bp_kernel(const BPArgs p) {
+    __shared__ float tile[BP_NZ][BP_ROWS][33];
     const Geom &g = p.g;
     const int tx = threadIdx.x, ty = threadIdx.y;
-    const int x0 = blockIdx.x * 32, y0 = blockIdx.y * 32, iz = blockIdx.z;
-    const int ix = x0 + tx;
+    const int x0 = blockIdx.x * 32, y0 = blockIdx.y * BP_ROWS, z0 = blockIdx.z * BP_NZ;
+    const int ix = x0 + tx, iy = y0 + ty;
+    const bool active = ix < g.nx && iy < g.ny;
     const float sphi = __sinf(p.angle), cphi = __cosf(p.angle);
-    const int64_t slice = (int64_t)iz * g.nx * g.ny;
+    const int na = g.na;
+
+    float acc0[BP_NZ], acc1[BP_NZ];
 #pragma unroll
-    for (int k = 0; k < 4; k++) {
-        const int ly = ty + 8 * k, iy = y0 + ly;
+    for (int k = 0; k < BP_NZ; k++) { acc0[k] = 0.0f; acc1[k] = 0.0f; }
+
+    if (active) {
+        const BPColumn col = bp_column(ix, iy, cphi, sphi, g);
+        // rows of each slice: first row, count (BP_WB + 1 = more than BP_WB),
+        // row weights, box
+        int ib0[BP_NZ], nbk[BP_NZ];
+        float wb[BP_NZ][BP_WB], bmn[BP_NZ], bmx[BP_NZ];
+#pragma unroll
+        for (int k = 0; k < BP_NZ; k++) {
+            nbk[k] = 0;
+            ib0[k] = 0;
+            bmn[k] = 0.0f;
+            bmx[k] = 0.0f;
+#pragma unroll
+            for (int j = 0; j < BP_WB; j++) wb[k][j] = 0.0f;
+            const int iz = z0 + k;
+            if (iz < g.nz) {
+                bp_rows(col, iz, g, bmn[k], bmx[k]);
+                const float blim = ((float)g.nb < bmx[k]) ? (float)g.nb : bmx[k];  // MIN(nb, b_max)
+                ib0[k] = max(0, (int)floorf(fmaxf(bmn[k], -1.0f)));
+                // rows ib >= ib0 with (float)ib < blim, i.e. ib < ceil(blim)
+                // (blim <= nb, so every row index is exact in float; a NaN
+                // converts to 0 and gives no rows, as the loop test would)
+                nbk[k] = min(BP_WB + 1, max(0, (int)ceilf(blim) - ib0[k]));
+#pragma unroll
+                for (int j = 0; j < BP_WB; j++) {
+                    const int ib = ib0[k] + j;
+                    wb[k][j] = fminf(ib + 1.0f, bmx[k]) - fmaxf(ib + 0.0f, bmn[k]);
+                }
+            }
+        }
+        const float alim = ((float)na < col.amax) ? (float)na : col.amax;  // MIN(na, a_max)
+        const int ia0 = max(0, (int)floorf(fmaxf(col.amin, -1.0f)));
+        for (int ia = ia0; (float)ia < alim; ia++) {
+            const float wa = fminf(ia + 1.0f, col.amax) - fmaxf(ia + 0.0f, col.amin);
+#pragma unroll
+            for (int k = 0; k < BP_NZ; k++) {
+                if (nbk[k] <= BP_WB) {
+#pragma unroll
+                    for (int j = 0; j < BP_WB; j++) {
+                        if (j < nbk[k]) {
+                            const float w = __fmul_rn(wa, wb[k][j]);
+                            const int pix = ia + (ib0[k] + j) * na;
+                            if (K == 1) {
+                                acc0[k] = __fmaf_rn(w, __ldg(p.proj + pix), acc0[k]);
+                            } else {
+                                const float2 v = __ldg(p.pair + pix);
+                                acc0[k] = __fmaf_rn(w, v.x, acc0[k]);
+                                acc1[k] = __fmaf_rn(w, v.y, acc1[k]);
+                            }
+                        }
+                    }
+                } else {
+                    const float blim = ((float)g.nb < bmx[k]) ? (float)g.nb : bmx[k];
+                    for (int ib = ib0[k]; (float)ib < blim; ib++) {
+                        const float w =
+                            __fmul_rn(wa, fminf(ib + 1.0f, bmx[k]) - fmaxf(ib + 0.0f, bmn[k]));
+                        const int pix = ia + ib * na;
+                        if (K == 1) {
+                            acc0[k] = __fmaf_rn(w, __ldg(p.proj + pix), acc0[k]);
+                        } else {
+                            const float2 v = __ldg(p.pair + pix);
+                            acc0[k] = __fmaf_rn(w, v.x, acc0[k]);
+                            acc1[k] = __fmaf_rn(w, v.y, acc1[k]);
+                        }
+                    }
+                }
+            }
+        }
+    }
+
+    const int64_t plane = (int64_t)g.nx * g.ny;
+#pragma unroll
+    for (int k = 0; k < BP_NZ; k++) {
+        const int iz = z0 + k;
         float val = 0.0f;
-        if (ix < g.nx && iy < g.ny) {
-            const BPBox box = bp_box(ix, iy, iz, cphi, sphi, g);
-            float acc[2] = {0.0f, 0.0f};
-            bp_gather<K>(box, p.proj, p.pair, g, acc);
-            const int64_t id = ix + (int64_t)iy * g.nx + slice;
+        if (active && iz < g.nz) {
+            const int64_t id = ix + (int64_t)iy * g.nx + iz * plane;
             if (MODE == BP_PLAIN) {
-                val = acc[0];
+                val = acc0[k];
                 p.out[id] = val;
             } else {
-                float q = acc[0] / acc[1];              // cu_division.cu:20
+                float q = acc0[k] / acc1[k];            // cu_division.cu:20
                 if (isnan(q) || isinf(q)) q = 0.0f;     // :21-24
                 if (MODE == BP_DIV) {
                     val = q;
@@ -132,16 +206,20 @@ __global__ void __launch_bounds__(256) bp_kernel(const BPArgs p) {
                 }
             }
         }
-        if (MODE == BP_DIV_ADD) tile[ly][tx] = val;
+        if (MODE == BP_DIV_ADD) tile[k][ty][tx] = val;
     }
     if (MODE == BP_DIV_ADD && p.outT != nullptr) {
         __syncthreads();
-        // transposed store: outT[iy + ix*ny + iz*nx*ny]
-        const int iyT = y0 + tx;
+        // transposed store outT[iy + ix*ny + iz*nx*ny]: 8 consecutive iy per ix
+        const int t = ty * 32 + tx;
+        const int lx = t / BP_ROWS, ly = t % BP_ROWS;
+        const int ixT = x0 + lx, iyT = y0 + ly;
+        if (ixT < g.nx && iyT < g.ny) {
 #pragma unroll
-        for (int k = 0; k < 4; k++) {
-            const int lx = ty + 8 * k, ixT = x0 + lx;
-            if (ixT < g.nx && iyT < g.ny) p.outT[iyT + (int64_t)ixT * g.ny + slice] = tile[tx][lx];
+            for (int k = 0; k < BP_NZ; k++) {
+                const int iz = z0 + k;
+                if (iz < g.nz) p.outT[iyT + (int64_t)ixT * g.ny + iz * plane] = tile[k][ly][lx];
+            }
         }
     }
 }

@@ -45,7 +45,7 @@ int scratch_of_current_device(float **out) {
         MC_CHECK_CUDA(cudaGetSymbolAddress(&p, g_noalloc_volT));
         cudaFuncAttributes fa;
         MC_CHECK_CUDA(cudaFuncGetAttributes(&fa, transpose_kernel<float, float>));
-        MC_CHECK_CUDA(cudaFuncGetAttributes(&fa, fp_kernel<1, false, SUM_REF, float>));
+        MC_CHECK_CUDA(cudaFuncGetAttributes(&fa, fp_ref_kernel<1, false, float>));
         g_scratch[dev] = static_cast<float *>(p);
     }
     *out = g_scratch[dev];
@@ -88,8 +88,8 @@ MC_EXPORT int mcsart_projection_noalloc(void *stream, float *d_proj, const float
     a.angles = nullptr;
     a.mode = FP_PLAIN;
     a.out = d_proj;
-    const dim3 grid(div_up(na, 32), div_up(nb, 8), 1), block(32, 8);
-    fp_kernel<1, false, SUM_REF, float><<<grid, block, 0, s>>>(a);
+    const dim3 grid(div_up(na, FPC_COLS), div_up(nb, FPC_ROWS), 1);
+    fp_ref_kernel<1, false, float><<<grid, dim3(FPC_THREADS), 0, s>>>(a);
     MC_CHECK_CUDA(cudaGetLastError());
     return MCSART_OK;
 }

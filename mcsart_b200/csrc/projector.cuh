@@ -246,6 +246,295 @@ template <typename VT, int K, typename MT = VT> struct FPArgs {
     double2 *norm_part; // per-block (sum b^2, sum r^2)
 };
 
+// ------------------------------------------------------------------------
+// Column-shared projector for the reference summation order (SUM_REF).
+//
+// Every ray of one detector column ia has the same in-plane geometry: the
+// driving axis, the four edge ratios and so, per slab, the in-plane voxel
+// range U1..U2 and weights w_u (only the axial part depends on the row ib,
+// through z2).  A block of FPC_COLS columns x FPC_ROWS rows computes the
+// in-plane part once per (column, slab) into shared memory, FPC_CHUNK slabs
+// at a time, and every ray then adds its axial part and its terms in the
+// reference's order.  The per-ray arithmetic is unchanged, so the sums are
+// bitwise those of the per-ray form (and of the reference kernel).
+constexpr int FPC_COLS = 16, FPC_ROWS = 8, FPC_THREADS = FPC_COLS * FPC_ROWS;
+constexpr int FPC_CHUNK = 32;
+// Slabs per group in the 2x2 fast path.
+#ifndef MCSART_FP_GROUP
+#define MCSART_FP_GROUP 2
+#endif
+constexpr int FPC_GROUP = MCSART_FP_GROUP;
+
+// In-plane footprint of one slab.  U2 - U1 <= 1: (a, b) = weights of voxels
+// U1 and U1 + 1; otherwise (a, b) = (ui1, ui2), the footprint edges.
+struct SlabU {
+    int U1, U2;
+    float a, b;
+};
+
+// :52-63 / :105-116 for slab d of the ray's column.
+__device__ __forceinline__ SlabU slab_u(const RayGeom &r, int d) {
+    const float dc = __fsub_rn(__fsub_rn(__fadd_rn((float)d, 0.5f), r.d_half), r.src_d);
+    const float c0 = __fadd_rn(__fmaf_rn(r.r0, dc, r.u_off), r.u_half);
+    const float c1 = __fadd_rn(__fmaf_rn(r.r1, dc, r.u_off), r.u_half);
+    const float c2 = __fadd_rn(__fmaf_rn(r.r2, dc, r.u_off), r.u_half);
+    const float c3 = __fadd_rn(__fmaf_rn(r.r3, dc, r.u_off), r.u_half);
+    const float ui1 = fminf(fminf(c0, c1), fminf(c2, c3));
+    const float ui2 = fmaxf(fmaxf(c0, c1), fmaxf(c2, c3));
+    SlabU e;
+    e.U1 = (int)floorf(ui1);
+    e.U2 = (int)floorf(ui2);
+    if (e.U2 - e.U1 <= 1) {
+        const float du = __fsub_rn(ui2, ui1);  // :83 / :136
+        const float fu0 = (float)e.U1, fu1 = (float)(e.U1 + 1);
+        e.a = __fdiv_rn(__fsub_rn(fminf(__fadd_rn(fu0, 1.0f), ui2), fmaxf(fu0, ui1)), du);
+        e.b = __fdiv_rn(__fsub_rn(fminf(__fadd_rn(fu1, 1.0f), ui2), fmaxf(fu1, ui1)), du);
+    } else {
+        e.a = ui1;
+        e.b = ui2;
+    }
+    return e;
+}
+
+// A 2x2 footprint window (U1, U1+1) x (Z1, Z1+1) of one slab: weights,
+// clamped (always in-bounds) addresses and which of the four voxels the
+// reference's loops visit (:80-88 / :133-141).
+struct SlabZ {
+    float wu0, wu1, wz0, wz1;
+    int a00, a01, a10, a11;
+    bool p00, p01, p10, p11;
+};
+
+// Axial part of slab d for this ray; true (and w filled) if the footprint is
+// a 2x2 window.  Voxel indices are 32-bit: volumes are validated to hold
+// fewer than 2^31 voxels (the reference indexes with int as well).
+__device__ __forceinline__ bool slab_window(const RayGeom &r, const Geom &g, const SlabU &e, int d,
+                                            int su, int sd, int sz, float z_half, SlabZ &w) {
+    const float dc = __fsub_rn(__fsub_rn(__fadd_rn((float)d, 0.5f), r.d_half), r.src_d);
+    // :71-77 / :124-130 ("ratio * xc + z1 + nz / 2", z1 = 0)
+    const float cz0 = __fadd_rn(__fmul_rn(r.rz0, dc), z_half);
+    const float cz1 = __fadd_rn(__fmul_rn(r.rz1, dc), z_half);
+    const float zi1 = fminf(cz0, cz1), zi2 = fmaxf(cz0, cz1);
+    const int Z1 = (int)floorf(zi1), Z2 = (int)floorf(zi2);
+    const float dz = __fsub_rn(zi2, zi1);
+    const int U1 = e.U1, U2 = e.U2;
+    const bool u0 = U1 >= 0 && U1 <= r.nu - 1;
+    const bool u1 = U1 + 1 <= U2 && U1 + 1 >= 0 && U1 + 1 <= r.nu - 1;
+    const bool z0 = Z1 >= 0 && Z1 <= g.nz - 1;
+    const bool z1 = Z1 + 1 <= Z2 && Z1 + 1 >= 0 && Z1 + 1 <= g.nz - 1;
+    w.p00 = u0 && z0;
+    w.p01 = u0 && z1;
+    w.p10 = u1 && z0;
+    w.p11 = u1 && z1;
+    w.wu0 = e.a;
+    w.wu1 = e.b;
+    const float fz0 = (float)Z1, fz1 = (float)(Z1 + 1);
+    w.wz0 = __fdiv_rn(__fsub_rn(fminf(__fadd_rn(fz0, 1.0f), zi2), fmaxf(fz0, zi1)), dz);
+    w.wz1 = __fdiv_rn(__fsub_rn(fminf(__fadd_rn(fz1, 1.0f), zi2), fmaxf(fz1, zi1)), dz);
+    const int cu0 = min(max(U1, 0), r.nu - 1), cu1 = min(max(U1 + 1, 0), r.nu - 1);
+    const int cz0i = min(max(Z1, 0), g.nz - 1), cz1i = min(max(Z1 + 1, 0), g.nz - 1);
+    const int r0 = cu0 * su + d * sd, r1 = cu1 * su + d * sd;
+    w.a00 = r0 + cz0i * sz;
+    w.a01 = r0 + cz1i * sz;
+    w.a10 = r1 + cz0i * sz;
+    w.a11 = r1 + cz1i * sz;
+    return U2 - U1 <= 1 && Z2 - Z1 <= 1;
+}
+
+// One slab of one ray, any footprint: the 2x2 window with predication or the
+// reference's loops (:80-88 / :133-141).
+template <int K, bool ONES, typename VT>
+__device__ __forceinline__ void fp_slab(const RayGeom &r, const Geom &g, const SlabU &e, int d,
+                                        const VT *const *base, int su, int sd, int sz,
+                                        float z_half, float *acc, float &accw) {
+    SlabZ w;
+    if (slab_window(r, g, e, d, su, sd, sz, z_half, w)) {
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            if (w.p00) acc[k] = __fmaf_rn(__fmul_rn(ldv(base[k], w.a00), w.wu0), w.wz0, acc[k]);
+            if (w.p01) acc[k] = __fmaf_rn(__fmul_rn(ldv(base[k], w.a01), w.wu0), w.wz1, acc[k]);
+            if (w.p10) acc[k] = __fmaf_rn(__fmul_rn(ldv(base[k], w.a10), w.wu1), w.wz0, acc[k]);
+            if (w.p11) acc[k] = __fmaf_rn(__fmul_rn(ldv(base[k], w.a11), w.wu1), w.wz1, acc[k]);
+        }
+        if (ONES) {
+            if (w.p00) accw = __fmaf_rn(w.wu0, w.wz0, accw);
+            if (w.p01) accw = __fmaf_rn(w.wu0, w.wz1, accw);
+            if (w.p10) accw = __fmaf_rn(w.wu1, w.wz0, accw);
+            if (w.p11) accw = __fmaf_rn(w.wu1, w.wz1, accw);
+        }
+        return;
+    }
+    const float dc = __fsub_rn(__fsub_rn(__fadd_rn((float)d, 0.5f), r.d_half), r.src_d);
+    const float cz0 = __fadd_rn(__fmul_rn(r.rz0, dc), z_half);
+    const float cz1 = __fadd_rn(__fmul_rn(r.rz1, dc), z_half);
+    const float zi1 = fminf(cz0, cz1), zi2 = fmaxf(cz0, cz1);
+    const int Z1 = (int)floorf(zi1), Z2 = (int)floorf(zi2);
+    const float dz = __fsub_rn(zi2, zi1);
+    const int U1 = e.U1, U2 = e.U2;
+    const bool fast_u = U2 - U1 <= 1;
+    const int u_lo = max(0, U1), u_hi = min(r.nu - 1, U2);
+    const int z_lo = max(0, Z1), z_hi = min(g.nz - 1, Z2);
+    const float ui1 = e.a, ui2 = e.b;
+    const float du = fast_u ? 0.0f : __fsub_rn(ui2, ui1);
+    for (int u = u_lo; u <= u_hi; u++) {
+        const float wu = fast_u ? (u == U1 ? e.a : e.b)
+                                : __fdiv_rn(__fsub_rn(fminf(__fadd_rn((float)u, 1.0f), ui2),
+                                                      fmaxf((float)u, ui1)), du);
+        const int rowa = u * su + d * sd;
+        for (int z = z_lo; z <= z_hi; z++) {
+            const float wz = __fdiv_rn(__fsub_rn(fminf(__fadd_rn((float)z, 1.0f), zi2),
+                                                 fmaxf((float)z, zi1)), dz);
+            const int a = rowa + z * sz;
+#pragma unroll
+            for (int k = 0; k < K; k++)
+                acc[k] = __fmaf_rn(__fmul_rn(ldv(base[k], a), wu), wz, acc[k]);
+            if (ONES) accw = __fmaf_rn(wu, wz, accw);
+        }
+    }
+}
+
+// blockDim = FPC_THREADS: thread t is column t % FPC_COLS, row t / FPC_COLS;
+// gridDim = (ceil(na/FPC_COLS), ceil(nb/FPC_ROWS), views).
+template <int K, bool ONES, typename VT, typename MT = VT>
+__global__ void __launch_bounds__(FPC_THREADS) fp_ref_kernel(const FPArgs<VT, K, MT> p) {
+    __shared__ SlabU sm_u[FPC_CHUNK][FPC_COLS];
+    __shared__ double2 sm_norm[FPC_THREADS / 32];
+    const Geom &g = p.g;
+    const int t = threadIdx.x, col = t % FPC_COLS, row = t / FPC_COLS;
+    const int ia = blockIdx.x * FPC_COLS + col, ib = blockIdx.y * FPC_ROWS + row;
+    const bool col_ok = ia < g.na;
+    const bool active = col_ok && ib < g.nb;
+    const float angle = p.angles ? p.angles[blockIdx.z] : p.angle;
+    const float cphi = cosf(angle), sphi = sinf(angle);  // :23-24
+    // rows past the detector still compute their column's in-plane part
+    const RayGeom r = ray_geom(cphi, sphi, col_ok ? ia : 0, min(ib, g.nb - 1), g);
+
+    const VT *base[K];
+    int su, sd;
+    const int sz = g.nx * g.ny;
+    if (r.xdrive) {
+        if (p.vol.tr[0] != nullptr) {
+#pragma unroll
+            for (int k = 0; k < K; k++) base[k] = p.vol.tr[k];
+            su = 1; sd = g.ny;
+        } else {
+#pragma unroll
+            for (int k = 0; k < K; k++) base[k] = p.vol.std[k];
+            su = g.nx; sd = 1;
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < K; k++) base[k] = p.vol.std[k];
+        su = 1; sd = g.nx;
+    }
+    const float z_half = (float)(g.nz / 2);
+    float acc[K], accw = 0.0f;
+#pragma unroll
+    for (int k = 0; k < K; k++) acc[k] = 0.0f;
+
+    const int nd_max = max(g.nx, g.ny);
+    for (int d0 = 0; d0 < nd_max; d0 += FPC_CHUNK) {
+        for (int j = row; j < FPC_CHUNK; j += FPC_ROWS) {
+            const int d = d0 + j;
+            SlabU e;
+            e.U1 = 0; e.U2 = -1; e.a = 0.0f; e.b = 0.0f;
+            if (col_ok && d < r.nd) e = slab_u(r, d);
+            sm_u[j][col] = e;
+        }
+        __syncthreads();
+        const int dn = active ? min(FPC_CHUNK, r.nd - d0) : 0;
+        int j = 0;
+        // groups of FPC_GROUP slabs whose footprints are all 2x2 windows: the
+        // set-up and the (always in-bounds) loads of the whole group come
+        // first, then the terms enter the sums in the reference's order, so
+        // that a warp waits for memory once per group instead of per slab
+        for (; j + FPC_GROUP <= dn; j += FPC_GROUP) {
+            SlabZ w[FPC_GROUP];
+            bool all_fast = true;
+#pragma unroll
+            for (int q = 0; q < FPC_GROUP; q++)
+                all_fast &= slab_window(r, g, sm_u[j + q][col], d0 + j + q, su, sd, sz, z_half, w[q]);
+            if (all_fast) {
+                float v[FPC_GROUP][K][4];
+#pragma unroll
+                for (int q = 0; q < FPC_GROUP; q++)
+#pragma unroll
+                    for (int k = 0; k < K; k++) {
+                        v[q][k][0] = ldv(base[k], w[q].a00);
+                        v[q][k][1] = ldv(base[k], w[q].a01);
+                        v[q][k][2] = ldv(base[k], w[q].a10);
+                        v[q][k][3] = ldv(base[k], w[q].a11);
+                    }
+#pragma unroll
+                for (int q = 0; q < FPC_GROUP; q++) {
+                    const SlabZ &x = w[q];
+#pragma unroll
+                    for (int k = 0; k < K; k++) {
+                        if (x.p00) acc[k] = __fmaf_rn(__fmul_rn(v[q][k][0], x.wu0), x.wz0, acc[k]);
+                        if (x.p01) acc[k] = __fmaf_rn(__fmul_rn(v[q][k][1], x.wu0), x.wz1, acc[k]);
+                        if (x.p10) acc[k] = __fmaf_rn(__fmul_rn(v[q][k][2], x.wu1), x.wz0, acc[k]);
+                        if (x.p11) acc[k] = __fmaf_rn(__fmul_rn(v[q][k][3], x.wu1), x.wz1, acc[k]);
+                    }
+                    if (ONES) {
+                        if (x.p00) accw = __fmaf_rn(x.wu0, x.wz0, accw);
+                        if (x.p01) accw = __fmaf_rn(x.wu0, x.wz1, accw);
+                        if (x.p10) accw = __fmaf_rn(x.wu1, x.wz0, accw);
+                        if (x.p11) accw = __fmaf_rn(x.wu1, x.wz1, accw);
+                    }
+                }
+            } else {
+#pragma unroll 1
+                for (int q = 0; q < FPC_GROUP; q++)
+                    fp_slab<K, ONES, VT>(r, g, sm_u[j + q][col], d0 + j + q, base, su, sd, sz, z_half,
+                                         acc, accw);
+            }
+        }
+        for (; j < dn; j++)
+            fp_slab<K, ONES, VT>(r, g, sm_u[j][col], d0 + j, base, su, sd, sz, z_half, acc, accw);
+        __syncthreads();
+    }
+
+    const int64_t pix = ia + (int64_t)ib * g.na;
+    double nb2 = 0.0, nr2 = 0.0;
+    if (active) {
+        if (p.mode == FP_PLAIN) {
+            p.out[pix + (int64_t)blockIdx.z * g.na * g.nb] = acc[0];
+        } else {
+            const float b = ldv(p.meas, pix);
+            // AUMISART.cu:206 host_add(proj, proj_temp, -1): proj += proj_temp * -1
+            float res = __fmaf_rn(acc[0], -1.0f, b);
+            float ones = ONES ? accw : 0.0f;
+            if (p.mode == FP_MOTION) {
+                res = __fmaf_rn(acc[K > 1 ? 1 : 0], 1.0f, res);  // AUMISART.cu:260, + FP(img0)
+                if (K >= 3) ones = acc[K - 1];                   // FP(initial2(...)), :267-268
+            }
+            if (p.resid) p.resid[pix] = res;
+            p.bp_in[pix] = make_float2(res, ones);
+            nb2 = (double)b * (double)b;
+            nr2 = (double)res * (double)res;
+        }
+    }
+    if (p.mode == FP_PLAIN) return;
+    // block partial of the two squared norms, fixed-order reduction
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        nb2 += __shfl_down_sync(0xffffffffu, nb2, off);
+        nr2 += __shfl_down_sync(0xffffffffu, nr2, off);
+    }
+    if ((t & 31) == 0) sm_norm[t >> 5] = make_double2(nb2, nr2);
+    __syncthreads();
+    if (t == 0) {
+        double tb = 0.0, tr = 0.0;
+        for (int w = 0; w < FPC_THREADS / 32; w++) {
+            tb += sm_norm[w].x;
+            tr += sm_norm[w].y;
+        }
+        p.norm_part[blockIdx.y * gridDim.x + blockIdx.x] = make_double2(tb, tr);
+    }
+}
+
+// Per-ray projector, used for the split summation modes (the engine launches
+// fp_ref_kernel for SUM_REF).
 // Launch shapes.  SUM_REF: blockDim (32, 8), one ray per thread, 32 columns x
 // 8 rows per block, gridDim (ceil(na/32), ceil(nb/8), views).  Split modes:
 // blockDim (32, groups), threadIdx.y = slab group of the same 32 rays,

@@ -88,10 +88,10 @@ template <typename ST, int INTERP, int SUM> struct Runner {
         : ctx(c), S(*c->driver), P(p), opt(o) {
         V = nvox(P.g.nx, P.g.ny, P.g.nz);
         NP = (int64_t)P.g.na * P.g.nb;
-        fp_bx = (int)div_up(P.g.na, 32);
-        fp_by = SUM == SUM_REF ? (int)div_up(P.g.nb, 8) : P.g.nb;
+        fp_bx = SUM == SUM_REF ? (int)div_up(P.g.na, FPC_COLS) : (int)div_up(P.g.na, 32);
+        fp_by = SUM == SUM_REF ? (int)div_up(P.g.nb, FPC_ROWS) : P.g.nb;
         fp_blocks = fp_bx * fp_by;
-        groups = SUM == SUM_REF ? 8
+        groups = SUM == SUM_REF ? 1
                  : opt.fp_groups > 0 ? std::min(opt.fp_groups, 8)
                                      : fp_auto_groups(fp_blocks, std::max(P.g.nx, P.g.ny));
         for (int v = 0; v < P.n_views; v++) views_img.push_back(v);
@@ -150,10 +150,14 @@ template <typename ST, int INTERP, int SUM> struct Runner {
         a.resid = (mode == FP_IMAGE && P.resid) ? P.resid + (int64_t)v * NP : nullptr;
         a.bp_in = S.pairs.as<float2>();
         a.norm_part = S.norm_part.as<double2>() + (int64_t)k * fp_blocks;
-        const dim3 grid(fp_bx, fp_by, 1), block(32, groups);
-        const size_t smem = SUM == SUM_REF ? 0 : (size_t)groups * (K + 1) * 32 * sizeof(float);
+        const dim3 grid(fp_bx, fp_by, 1);
         ctx->label = mode == FP_MOTION ? "fp_motion" : "fp_image";
-        MC_LAUNCH(ctx, (fp_kernel<K, ONES, SUM, VT, ST>), grid, block, smem, a);
+        if (SUM == SUM_REF) {
+            MC_LAUNCH(ctx, (fp_ref_kernel<K, ONES, VT, ST>), grid, dim3(FPC_THREADS), 0, a);
+        } else {
+            const size_t smem = (size_t)groups * (K + 1) * 32 * sizeof(float);
+            MC_LAUNCH(ctx, (fp_kernel<K, ONES, SUM, VT, ST>), grid, dim3(32, groups), smem, a);
+        }
         return MCSART_OK;
     }
 
@@ -166,7 +170,8 @@ template <typename ST, int INTERP, int SUM> struct Runner {
         b.lambda = P.lambda;
         b.out = out;
         b.outT = outT;
-        const dim3 grid(div_up(P.g.nx, 32), div_up(P.g.ny, 32), P.g.nz), block(32, 8);
+        const dim3 grid(div_up(P.g.nx, 32), div_up(P.g.ny, BP_ROWS), div_up(P.g.nz, BP_NZ)),
+            block(32, BP_ROWS);
         if (mode == BP_DIV) {
             ctx->label = "bp_div";
             MC_LAUNCH(ctx, (bp_kernel<2, BP_DIV>), grid, block, 0, b);
@@ -239,11 +244,11 @@ template <typename ST, int INTERP, int SUM> struct Runner {
             const float iflow = P.flows[0] - P.flows[v];
             ctx->label = "warp_back_add";
             if (hw) {
-                MC_LAUNCH(ctx, (warp_back_add_kernel<SrcTex, ST>), stream_blocks(V), 256, 0,
+                MC_LAUNCH(ctx, (warp_back_add_kernel<SrcTex, ST>), tile_grid(), dim3(32, 8), 0,
                           P.img, S.tv_img.surf, SrcTex{S.tv_ratio.tex}, f, g.nx, g.ny, g.nz,
                           ivolume, iflow, P.lambda);
             } else {
-                MC_LAUNCH(ctx, (warp_back_add_kernel<SrcLinear<float>, ST>), stream_blocks(V), 256,
+                MC_LAUNCH(ctx, (warp_back_add_kernel<SrcLinear<float>, ST>), tile_grid(), dim3(32, 8),
                           0, P.img, (cudaSurfaceObject_t)0,
                           SrcLinear<float>{S.ratio.as<float>()}, f, g.nx, g.ny, g.nz, ivolume,
                           iflow, P.lambda);

@@ -23,13 +23,25 @@ template <typename FT> struct Fields {
 };
 
 // Sample of `src` for output memory index id (any id in [0, nx*ny*nz)).
+// The reference indexes the warp's output in-slice transposed
+// (cu_deform.cu:82-85): memory position r = x + y*nx of a slice is treated as
+// (ix, iy) = (r / ny, r % ny).  For square slices that is (y, x).
+__device__ __forceinline__ void warp_coords(int x, int y, int nx, int ny, int &ix, int &iy) {
+    if (nx == ny) {
+        ix = y;
+        iy = x;
+    } else {
+        const int r = x + y * nx;
+        ix = r / ny;
+        iy = r - ix * ny;
+    }
+}
+
+// Sample of voxel id, whose in-slice transposed coordinates are (ix, iy, iz).
 template <typename SRC, typename FT>
-__device__ __forceinline__ float warp_sample(const SRC &src, const Fields<FT> &f, int64_t id,
-                                             int nx, int ny, int nz, float volume, float flow) {
-    const int64_t plane = (int64_t)nx * ny;
-    const int iz = (int)(id / plane);
-    const int64_t r = id - (int64_t)iz * plane;
-    const int ix = (int)(r / ny), iy = (int)(r - (int64_t)ix * ny);
+__device__ __forceinline__ float warp_sample_at(const SRC &src, const Fields<FT> &f, int64_t id,
+                                                int ix, int iy, int iz, int nx, int ny, int nz,
+                                                float volume, float flow) {
     // kernel_forwardDVF, cu_deform.cu:74-76
     const float mx = ldv(f.ax, id) * volume + ldv(f.bx, id) * flow;
     const float my = ldv(f.ay, id) * volume + ldv(f.by, id) * flow;
@@ -41,7 +53,16 @@ __device__ __forceinline__ float warp_sample(const SRC &src, const Fields<FT> &f
     return src.fetch(xi - 0.5f, yi - 0.5f, zi - 0.5f, nx, ny, nz);
 }
 
-// Drop-in host_deform: out[id] = warp(src)[id] for all id.
+template <typename SRC, typename FT>
+__device__ __forceinline__ float warp_sample(const SRC &src, const Fields<FT> &f, int64_t id,
+                                             int nx, int ny, int nz, float volume, float flow) {
+    const int64_t plane = (int64_t)nx * ny;
+    const int iz = (int)(id / plane);
+    const int r = (int)(id - (int64_t)iz * plane);
+    const int ix = r / ny, iy = r - ix * ny;
+    return warp_sample_at(src, f, id, ix, iy, iz, nx, ny, nz, volume, flow);
+}
+
 template <typename SRC>
 static __global__ void __launch_bounds__(256) deform_kernel(float *out, const SRC src,
                                                             Fields<float> f, int nx, int ny,
@@ -108,7 +129,9 @@ static __global__ void __launch_bounds__(256) warp_fwd_kernel(VT *dst, VT *dstT,
         float v = 0.0f;
         if (xm < nx && ym < ny) {
             const int64_t id = xm + (int64_t)ym * nx + slice;
-            v = warp_sample(src, f, id, nx, ny, nz, volume, flow);
+            int ix, iy;
+            warp_coords(xm, ym, nx, ny, ix, iy);
+            v = warp_sample_at(src, f, id, ix, iy, iz, nx, ny, nz, volume, flow);
             dst[id] = cvt<VT>(v);
         }
         tile[ly][tx] = v;
@@ -126,22 +149,27 @@ static __global__ void __launch_bounds__(256) warp_fwd_kernel(VT *dst, VT *dstT,
 // img[id] += lambda * warp(src)[id]  (AUMISART.cu:222-223).  With a surface,
 // the updated voxel is also written to the 3D array the next forward warp
 // samples through the texture unit.
+// blockDim (32, 8), 32x32 tiles of slice blockIdx.z (4 rows per thread).
 template <typename SRC, typename FT>
 static __global__ void __launch_bounds__(256) warp_back_add_kernel(
     float *img, cudaSurfaceObject_t img_surf, const SRC src, Fields<FT> f, int nx, int ny,
     int nz, float volume, float flow, float lambda) {
-    const int64_t n = nvox(nx, ny, nz), plane = (int64_t)nx * ny;
-    for (int64_t id = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; id < n;
-         id += (int64_t)gridDim.x * blockDim.x) {
-        const float w = warp_sample(src, f, id, nx, ny, nz, volume, flow);
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int xm = blockIdx.x * 32 + tx, iz = blockIdx.z;
+    const int64_t slice = (int64_t)iz * nx * ny;
+    if (xm >= nx) return;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const int ym = blockIdx.y * 32 + ty + 8 * k;
+        if (ym >= ny) break;
+        const int64_t id = xm + (int64_t)ym * nx + slice;
+        int ix, iy;
+        warp_coords(xm, ym, nx, ny, ix, iy);
+        const float w = warp_sample_at(src, f, id, ix, iy, iz, nx, ny, nz, volume, flow);
         const float v = __fmaf_rn(w, lambda, img[id]);  // cu_add.cu:17
         img[id] = v;
-        if (img_surf) {
-            const int z = (int)(id / plane);
-            const int64_t r = id - (int64_t)z * plane;
-            const int y = (int)(r / nx), x = (int)(r - (int64_t)y * nx);
-            surf3Dwrite(v, img_surf, x * (int)sizeof(float), y, z, cudaBoundaryModeZero);
-        }
+        if (img_surf)
+            surf3Dwrite(v, img_surf, xm * (int)sizeof(float), ym, iz, cudaBoundaryModeZero);
     }
 }
 
