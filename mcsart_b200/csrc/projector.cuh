@@ -287,8 +287,15 @@ __device__ __forceinline__ SlabU slab_u(const RayGeom &r, int d) {
     if (e.U2 - e.U1 <= 1) {
         const float du = __fsub_rn(ui2, ui1);  // :83 / :136
         const float fu0 = (float)e.U1, fu1 = (float)(e.U1 + 1);
-        e.a = __fdiv_rn(__fsub_rn(fminf(__fadd_rn(fu0, 1.0f), ui2), fmaxf(fu0, ui1)), du);
-        e.b = __fdiv_rn(__fsub_rn(fminf(__fadd_rn(fu1, 1.0f), ui2), fmaxf(fu1, ui1)), du);
+        const float n0 = __fsub_rn(fminf(__fadd_rn(fu0, 1.0f), ui2), fmaxf(fu0, ui1));
+        const float n1 = __fsub_rn(fminf(__fadd_rn(fu1, 1.0f), ui2), fmaxf(fu1, ui1));
+        const float y = mk_recip(du);
+        e.a = mk_div(n0, du, y);
+        e.b = mk_div(n1, du, y);
+        if (!(mk_den_ok(du) && mk_num_ok(n0) && mk_num_ok(n1))) {
+            e.a = __fdiv_rn(n0, du);
+            e.b = __fdiv_rn(n1, du);
+        }
     } else {
         e.a = ui1;
         e.b = ui2;
@@ -306,7 +313,7 @@ struct SlabZ {
 };
 
 // Axial part of slab d for this ray; true (and w filled) if the footprint is
-// a 2x2 window.  Voxel indices are 32-bit: volumes are validated to hold
+// a 2x2 window whose weights the branch-free division computed exactly.  Voxel indices are 32-bit: volumes are validated to hold
 // fewer than 2^31 voxels (the reference indexes with int as well).
 __device__ __forceinline__ bool slab_window(const RayGeom &r, const Geom &g, const SlabU &e, int d,
                                             int su, int sd, int sz, float z_half, SlabZ &w) {
@@ -329,8 +336,12 @@ __device__ __forceinline__ bool slab_window(const RayGeom &r, const Geom &g, con
     w.wu0 = e.a;
     w.wu1 = e.b;
     const float fz0 = (float)Z1, fz1 = (float)(Z1 + 1);
-    w.wz0 = __fdiv_rn(__fsub_rn(fminf(__fadd_rn(fz0, 1.0f), zi2), fmaxf(fz0, zi1)), dz);
-    w.wz1 = __fdiv_rn(__fsub_rn(fminf(__fadd_rn(fz1, 1.0f), zi2), fmaxf(fz1, zi1)), dz);
+    const float n0 = __fsub_rn(fminf(__fadd_rn(fz0, 1.0f), zi2), fmaxf(fz0, zi1));
+    const float n1 = __fsub_rn(fminf(__fadd_rn(fz1, 1.0f), zi2), fmaxf(fz1, zi1));
+    const float y = mk_recip(dz);
+    w.wz0 = mk_div(n0, dz, y);
+    w.wz1 = mk_div(n1, dz, y);
+    const bool exact = mk_den_ok(dz) && mk_num_ok(n0) && mk_num_ok(n1);
     const int cu0 = min(max(U1, 0), r.nu - 1), cu1 = min(max(U1 + 1, 0), r.nu - 1);
     const int cz0i = min(max(Z1, 0), g.nz - 1), cz1i = min(max(Z1 + 1, 0), g.nz - 1);
     const int r0 = cu0 * su + d * sd, r1 = cu1 * su + d * sd;
@@ -338,7 +349,8 @@ __device__ __forceinline__ bool slab_window(const RayGeom &r, const Geom &g, con
     w.a01 = r0 + cz1i * sz;
     w.a10 = r1 + cz0i * sz;
     w.a11 = r1 + cz1i * sz;
-    return U2 - U1 <= 1 && Z2 - Z1 <= 1;
+    // outside the division's checked range the caller takes the general path
+    return U2 - U1 <= 1 && Z2 - Z1 <= 1 && exact;
 }
 
 // One slab of one ray, any footprint: the 2x2 window with predication or the
