@@ -43,16 +43,9 @@ __device__ __forceinline__ BPColumn bp_column(int ix, int iy, float cphi, float 
     const float u = __fmaf_rn(yc, cphi, __fmul_rn(-xc, sphi));
     const float tl = t - 0.5f, tr = t + 0.5f, ul = u - 0.5f, ur = u + 0.5f;
     BPColumn c;
-    const float dl = tl + g.SO, dr = tr + g.SO, d0 = t + g.SO;
-    // SD / (x + SO) at the three distances (branch-free exact division)
-    c.rl = mk_div(g.SD, dl, mk_recip(dl));  // points ll and lr
-    c.rr = mk_div(g.SD, dr, mk_recip(dr));  // points rr and rl
-    c.r0 = mk_div(g.SD, d0, mk_recip(d0));  // top and bottom
-    if (!(mk_num_ok(g.SD) && mk_den_ok(dl) && mk_den_ok(dr) && mk_den_ok(d0))) {
-        c.rl = g.SD / dl;
-        c.rr = g.SD / dr;
-        c.r0 = g.SD / d0;
-    }
+    c.rl = g.SD / (tl + g.SO);  // points ll and lr
+    c.rr = g.SD / (tr + g.SO);  // points rr and rl
+    c.r0 = g.SD / (t + g.SO);   // top and bottom
     const float all = c.rl * ul, alr = c.rl * ur, arr = c.rr * ur, arl = c.rr * ul, at = c.r0 * u;
     const float amax = fmaxf(fmaxf(fmaxf(all, arr), fmaxf(alr, arl)), at);
     const float amin = fminf(fminf(fminf(all, arr), fminf(alr, arl)), at);
@@ -210,8 +203,7 @@ __global__ void __launch_bounds__(256, MCSART_BP_MINBLOCKS) bp_kernel(const BPAr
                 val = acc0[k];
                 p.out[id] = val;
             } else {
-                float q = mk_div(acc0[k], acc1[k], mk_recip(acc1[k]));  // cu_division.cu:20
-                if (!(mk_den_ok(acc1[k]) && mk_num_ok(acc0[k]))) q = acc0[k] / acc1[k];
+                float q = acc0[k] / acc1[k];            // cu_division.cu:20
                 if (isnan(q) || isinf(q)) q = 0.0f;     // :21-24
                 if (MODE == BP_DIV) {
                     val = q;

@@ -257,7 +257,16 @@ template <typename VT, int K, typename MT = VT> struct FPArgs {
 // at a time, and every ray then adds its axial part and its terms in the
 // reference's order.  The per-ray arithmetic is unchanged, so the sums are
 // bitwise those of the per-ray form (and of the reference kernel).
-constexpr int FPC_COLS = 16, FPC_ROWS = 8, FPC_THREADS = FPC_COLS * FPC_ROWS;
+#ifndef MCSART_FP_COLS
+#define MCSART_FP_COLS 16
+#endif
+#ifndef MCSART_FP_ROWS
+#define MCSART_FP_ROWS 8
+#endif
+constexpr int FPC_COLS = MCSART_FP_COLS, FPC_ROWS = MCSART_FP_ROWS;
+constexpr int FPC_THREADS = FPC_COLS * FPC_ROWS;
+// at least 512 threads per SM: lets the compiler use up to 128 registers
+constexpr int FPC_MIN_BLOCKS = 512 / FPC_THREADS;
 constexpr int FPC_CHUNK = 32;
 // Slabs per group in the 2x2 fast path.
 #ifndef MCSART_FP_GROUP
@@ -408,7 +417,7 @@ __device__ __forceinline__ void fp_slab(const RayGeom &r, const Geom &g, const S
 // blockDim = FPC_THREADS: thread t is column t % FPC_COLS, row t / FPC_COLS;
 // gridDim = (ceil(na/FPC_COLS), ceil(nb/FPC_ROWS), views).
 template <int K, bool ONES, typename VT, typename MT = VT>
-__global__ void __launch_bounds__(FPC_THREADS) fp_ref_kernel(const FPArgs<VT, K, MT> p) {
+__global__ void __launch_bounds__(FPC_THREADS, FPC_MIN_BLOCKS) fp_ref_kernel(const FPArgs<VT, K, MT> p) {
     __shared__ SlabU sm_u[FPC_CHUNK][FPC_COLS];
     __shared__ double2 sm_norm[FPC_THREADS / 32];
     const Geom &g = p.g;
