@@ -154,6 +154,9 @@ def algorithmic_bytes(p) -> dict:
         "motion_prep": 4 * V + 24 * V + 16 * V,
         # read ratio, img, read+write 6 fields
         "field_update": 8 * V + 48 * V,
+        # the two above in one pass: read ratio, img, read+write 6 fields,
+        # write img0, ones and their copies
+        "field_update_prep": 8 * V + 48 * V + 16 * V,
     }
 
 

@@ -49,7 +49,8 @@ __device__ __forceinline__ BPColumn bp_column(int ix, int iy, float cphi, float 
     const float all = c.rl * ul, alr = c.rl * ur, arr = c.rr * ur, arl = c.rr * ul, at = c.r0 * u;
     const float amax = fmaxf(fmaxf(fmaxf(all, arr), fmaxf(alr, arl)), at);
     const float amin = fminf(fminf(fminf(all, arr), fminf(alr, arl)), at);
-    float qmax = mk_div(amax, g.da, mk_recip(g.da)), qmin = mk_div(amin, g.da, mk_recip(g.da));
+    const float ya = mk_recip(g.da);
+    float qmax = mk_div(amax, g.da, ya), qmin = mk_div(amin, g.da, ya);
     if (!(mk_den_ok(g.da) && mk_num_ok(amax) && mk_num_ok(amin))) {
         qmax = amax / g.da;
         qmin = amin / g.da;

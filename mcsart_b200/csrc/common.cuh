@@ -121,9 +121,11 @@ __device__ __forceinline__ bool mk_den_ok(float b) {
     const float m = fabsf(b);
     return m >= 0x1p-20f && m < 0x1p20f;
 }
+// +0 is fine; -0 is not: the correction step returns +0 for -0 / b, b > 0,
+// where the compiler's division returns -0.
 __device__ __forceinline__ bool mk_num_ok(float a) {
     const float m = fabsf(a);
-    return m == 0.0f || (m >= 0x1p-80f && m <= 0x1p80f);
+    return __float_as_uint(a) == 0u || (m >= 0x1p-80f && m <= 0x1p80f);
 }
 
 __host__ __device__ inline int64_t nvox(int nx, int ny, int nz) { return (int64_t)nx * ny * nz; }
@@ -142,6 +144,10 @@ template <> __device__ __forceinline__ float ldv<__nv_bfloat16>(const __nv_bfloa
 template <> __device__ __forceinline__ float ldv<__half>(const __half *p, int64_t i) {
     return __half2float(p[i]);
 }
+// A storage-type value as float (a value, not a load).
+__device__ __forceinline__ float tof(float v) { return v; }
+__device__ __forceinline__ float tof(__nv_bfloat16 v) { return __bfloat162float(v); }
+__device__ __forceinline__ float tof(__half v) { return __half2float(v); }
 template <typename T> __device__ __forceinline__ T cvt(float v);
 template <> __device__ __forceinline__ float cvt<float>(float v) { return v; }
 template <> __device__ __forceinline__ __nv_bfloat16 cvt<__nv_bfloat16>(float v) {

@@ -276,6 +276,97 @@ static __global__ void __launch_bounds__(256) field_update_kernel(FT *ax, FT *ay
     }
 }
 
+// field_update_kernel for view v followed by motion_prep_kernel for the next
+// view, in one pass over the fields (square slices, nx == ny).  The block of
+// output tile A = (x0, y0) updates the fields on the transposed memory tile
+// A^T, which is exactly the set motion_prep reads for A, keeps the updated
+// values in shared memory and then computes img0 / ones of tile A for the
+// next view.  Every field voxel is updated by exactly one block, and the
+// arithmetic is that of the two kernels, so the results are bitwise theirs.
+template <typename FT, typename VT>
+static __global__ void __launch_bounds__(256) field_update_prep_kernel(
+    FT *ax, FT *ay, FT *az, FT *bx, FT *by, FT *bz, const float *img_temp, const float *img,
+    int nx, int ny, int nz, float nvd, float nfd, VT *img0, VT *img0T, VT *ones, VT *onesT,
+    float vd, float fd) {
+    __shared__ float ft[6][32][33];
+    __shared__ float rt[32][33];
+    __shared__ float o0[32][33], o1[32][33];
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int x0 = blockIdx.x * 32, y0 = blockIdx.y * 32, iz = blockIdx.z;
+    const int64_t slice = (int64_t)iz * nx * ny;
+    // ratio on tile A, x-fastest: rt[y - y0][x - x0]
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const int ly = ty + 8 * k, xx = x0 + tx, yy = y0 + ly;
+        rt[ly][tx] = (xx < nx && yy < ny) ? img_temp[xx + (int64_t)yy * nx + slice] : 0.0f;
+    }
+    __syncthreads();
+    // field update on A^T: voxel (x', y') = (y0 + tx, x0 + lx); its q is the
+    // ratio at the transposed index, i.e. at (x0 + lx, y0 + tx) of tile A
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const int lx = ty + 8 * k, xp = y0 + tx, yp = x0 + lx;
+        float n[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+        if (xp < nx && yp < ny) {
+            const int64_t id = xp + (int64_t)yp * nx + slice;
+            const Vox v{xp, yp, iz};
+            const float dfx = fwd_diff(img, id, v, nx, ny, nz, 1);
+            const float dfy = fwd_diff(img, id, v, nx, ny, nz, 2);
+            const float dfz = fwd_diff(img, id, v, nx, ny, nz, 3);
+            const float q = rt[tx][lx];
+            const FT nay = cvt<FT>(__fmaf_rn(q * nvd, dfx, ldv(ay, id)));
+            const FT nax = cvt<FT>(__fmaf_rn(q * nvd, dfy, ldv(ax, id)));
+            const FT naz = cvt<FT>(__fmaf_rn(q * nvd, dfz, ldv(az, id)));
+            const FT nby = cvt<FT>(__fmaf_rn(q * nfd, dfx, ldv(by, id)));
+            const FT nbx = cvt<FT>(__fmaf_rn(q * nfd, dfy, ldv(bx, id)));
+            const FT nbz = cvt<FT>(__fmaf_rn(q * nfd, dfz, ldv(bz, id)));
+            ay[id] = nay; ax[id] = nax; az[id] = naz;
+            by[id] = nby; bx[id] = nbx; bz[id] = nbz;
+            n[0] = tof(nay); n[1] = tof(nax); n[2] = tof(naz);
+            n[3] = tof(nby); n[4] = tof(nbx); n[5] = tof(nbz);
+        }
+#pragma unroll
+        for (int c = 0; c < 6; c++) ft[c][lx][tx] = n[c];
+    }
+    __syncthreads();
+    // motion_prep_kernel for tile A with the next view's weights
+    const int ix = x0 + tx;
+    const float s_ones = (-vd) + (-fd);
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const int ly = ty + 8 * k, iy = y0 + ly;
+        float a = 0.0f, b = 0.0f;
+        if (ix < nx && iy < ny) {
+            const int64_t id = ix + (int64_t)iy * nx + slice;
+            const Vox v{ix, iy, iz};
+            const float dfx = fwd_diff(img, id, v, nx, ny, nz, 1);
+            const float dfy = fwd_diff(img, id, v, nx, ny, nz, 2);
+            const float dfz = fwd_diff(img, id, v, nx, ny, nz, 3);
+            a = __fmaf_rn(ft[0][tx][ly] * vd, dfx, a);
+            a = __fmaf_rn(ft[1][tx][ly] * vd, dfy, a);
+            a = __fmaf_rn(ft[2][tx][ly] * vd, dfz, a);
+            a = __fmaf_rn(ft[3][tx][ly] * fd, dfx, a);
+            a = __fmaf_rn(ft[4][tx][ly] * fd, dfy, a);
+            a = __fmaf_rn(ft[5][tx][ly] * fd, dfz, a);
+            b = (dfx + dfy + dfz) * s_ones;  // cu_initial.cu:48
+            img0[id] = cvt<VT>(a);
+            ones[id] = cvt<VT>(b);
+        }
+        o0[ly][tx] = a;
+        o1[ly][tx] = b;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const int lx = ty + 8 * k, ixT = x0 + lx, iyT = y0 + tx;
+        if (ixT < nx && iyT < ny) {
+            const int64_t t = iyT + (int64_t)ixT * ny + slice;
+            img0T[t] = cvt<VT>(o0[tx][lx]);
+            onesT[t] = cvt<VT>(o1[tx][lx]);
+        }
+    }
+}
+
 // Norm ratios ||r_v|| / ||b_v|| from per-block partials (fixed order); one
 // warp per view.  Replaces the two cublasSnrm2 calls per view.
 static __global__ void norm_finalize_kernel(float *norm_out, const double2 *part, int n_blocks,

@@ -489,6 +489,28 @@ __global__ void __launch_bounds__(FPC_THREADS, FPC_MIN_BLOCKS) fp_ref_kernel(con
 #pragma unroll
                 for (int q = 0; q < FPC_GROUP; q++) {
                     const SlabZ &x = w[q];
+                    if (K == 1 && ONES) {
+                        // one volume and the weight sum: the two chains
+                        // interleaved term by term (measured faster here; the
+                        // per-volume order below is faster with three volumes)
+                        if (x.p00) {
+                            acc[0] = __fmaf_rn(__fmul_rn(v[q][0][0], x.wu0), x.wz0, acc[0]);
+                            accw = __fmaf_rn(x.wu0, x.wz0, accw);
+                        }
+                        if (x.p01) {
+                            acc[0] = __fmaf_rn(__fmul_rn(v[q][0][1], x.wu0), x.wz1, acc[0]);
+                            accw = __fmaf_rn(x.wu0, x.wz1, accw);
+                        }
+                        if (x.p10) {
+                            acc[0] = __fmaf_rn(__fmul_rn(v[q][0][2], x.wu1), x.wz0, acc[0]);
+                            accw = __fmaf_rn(x.wu1, x.wz0, accw);
+                        }
+                        if (x.p11) {
+                            acc[0] = __fmaf_rn(__fmul_rn(v[q][0][3], x.wu1), x.wz1, acc[0]);
+                            accw = __fmaf_rn(x.wu1, x.wz1, accw);
+                        }
+                        continue;
+                    }
 #pragma unroll
                     for (int k = 0; k < K; k++) {
                         if (x.p00) acc[k] = __fmaf_rn(__fmul_rn(v[q][k][0], x.wu0), x.wz0, acc[k]);

@@ -278,23 +278,41 @@ template <typename ST, int INTERP, int SUM> struct Runner {
         vol.tr[1] = S.img0T.as<ST>();
         vol.std[2] = S.ones.as<ST>();
         vol.tr[2] = S.onesT.as<ST>();
-        for (int k = 0; k < (int)views_mot.size(); k++) {
+        // square slices: each view's field update and the next view's prep
+        // run as one kernel (one pass over the fields)
+        const bool fuse = g.nx == g.ny;
+        const int nm = (int)views_mot.size();
+        for (int k = 0; k < nm; k++) {
             const int v = views_mot[k];
             const float vd = P.volumes[v] - P.volumes[v - 1];  // :249-250
             const float fd = P.flows[v] - P.flows[v - 1];
-            ctx->label = "motion_prep";
-            MC_LAUNCH(ctx, (motion_prep_kernel<ST, ST>), tile_grid(), dim3(32, 8), 0,
-                      S.img0.as<ST>(), S.img0T.as<ST>(), S.ones.as<ST>(), S.onesT.as<ST>(),
-                      (const float *)P.img, f, g.nx, g.ny, g.nz, vd, fd);
+            if (!fuse || k == 0) {
+                ctx->label = "motion_prep";
+                MC_LAUNCH(ctx, (motion_prep_kernel<ST, ST>), tile_grid(), dim3(32, 8), 0,
+                          S.img0.as<ST>(), S.img0T.as<ST>(), S.ones.as<ST>(), S.onesT.as<ST>(),
+                          (const float *)P.img, f, g.nx, g.ny, g.nz, vd, fd);
+            }
             MC_TRY((launch_fp<3, false, ST>(vol, v, k, FP_MOTION)));
             MC_TRY(launch_bp(v, BP_DIV, S.ratio.as<float>(), nullptr));
             const float nvd = P.volumes[v - 1] - P.volumes[v];  // :272-277
             const float nfd = P.flows[v - 1] - P.flows[v];
-            ctx->label = "field_update";
-            MC_LAUNCH(ctx, (field_update_kernel<ST>), tile_grid(), dim3(32, 8), 0, fw, fw + V,
-                      fw + 2 * V, fw + 3 * V, fw + 4 * V, fw + 5 * V,
-                      (const float *)S.ratio.as<float>(), (const float *)P.img, g.nx, g.ny, g.nz,
-                      nvd, nfd);
+            if (fuse && k + 1 < nm) {
+                const int vn = views_mot[k + 1];
+                const float vdn = P.volumes[vn] - P.volumes[vn - 1];
+                const float fdn = P.flows[vn] - P.flows[vn - 1];
+                ctx->label = "field_update_prep";
+                MC_LAUNCH(ctx, (field_update_prep_kernel<ST, ST>), tile_grid(), dim3(32, 8), 0,
+                          fw, fw + V, fw + 2 * V, fw + 3 * V, fw + 4 * V, fw + 5 * V,
+                          (const float *)S.ratio.as<float>(), (const float *)P.img, g.nx, g.ny,
+                          g.nz, nvd, nfd, S.img0.as<ST>(), S.img0T.as<ST>(), S.ones.as<ST>(),
+                          S.onesT.as<ST>(), vdn, fdn);
+            } else {
+                ctx->label = "field_update";
+                MC_LAUNCH(ctx, (field_update_kernel<ST>), tile_grid(), dim3(32, 8), 0, fw, fw + V,
+                          fw + 2 * V, fw + 3 * V, fw + 4 * V, fw + 5 * V,
+                          (const float *)S.ratio.as<float>(), (const float *)P.img, g.nx, g.ny,
+                          g.nz, nvd, nfd);
+            }
         }
         return finalize_norms(S.views_motion.as<int>(), (int)views_mot.size());
     }

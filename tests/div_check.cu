@@ -39,9 +39,15 @@ __global__ void check_random(unsigned long long *bad, uint32_t seed, int n_per) 
         const float fz = floorf(lo) + (float)(r2 & 1);
         const float a = __fsub_rn(fminf(__fadd_rn(fz, 1.0f), hi), fmaxf(fz, lo));
         const float b = __fsub_rn(hi, lo);
-        if (mk_den_ok(b) && mk_num_ok(a) &&
-            __float_as_uint(mk_div(a, b, mk_recip(b))) != __float_as_uint(__fdiv_rn(a, b)))
-            atomicAdd(&bad[2], 1ull);
+        // both signs of the numerator (-0 is outside the accepted range)
+        if (mk_den_ok(b)) {
+            const float y = mk_recip(b);
+            if (mk_num_ok(a) && __float_as_uint(mk_div(a, b, y)) != __float_as_uint(__fdiv_rn(a, b)))
+                atomicAdd(&bad[2], 1ull);
+            if (mk_num_ok(-a) &&
+                __float_as_uint(mk_div(-a, b, y)) != __float_as_uint(__fdiv_rn(-a, b)))
+                atomicAdd(&bad[2], 1ull);
+        }
         const float a2 = __uint_as_float(((uint32_t)(107 + (r1 % 40)) << 23) | (r2 >> 9)) *
                          ((r3 & 1) ? -1.0f : 1.0f);
         const float b2 = __uint_as_float(((uint32_t)(107 + (r3 % 40)) << 23) | (r1 >> 9));
