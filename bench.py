@@ -47,7 +47,7 @@ def parse():
                     help="views per pass in the CPU sample (0 = auto)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
-                    help="skip the mixed-precision and fast-FP32 side measurements")
+                    help="skip the 16-bit-storage and split-sum side measurements")
     ap.add_argument("--profile-steps", type=int, default=0,
                     help="only run this many untimed steps inside the NVTX range "
                          "'mcsart_step' (for a profiler's launch list) and exit")
@@ -158,6 +158,17 @@ def algorithmic_bytes(p) -> dict:
         # write img0, ones and their copies
         "field_update_prep": 8 * V + 48 * V + 16 * V,
     }
+
+
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per launch of the
+# c2 workload's kernels, from one `ncu --set full` capture of each (cold cache,
+# FP32 storage); summaries with the commands are kept under profiles/.
+NCU_DRAM_BYTES_C2 = {
+    "fp_motion": 15439360 + 0,
+    "fp_image": 5301248 + 0,
+    "bp_div": 409856 + 0,
+    "field_update_prep": 50349824 + 5771264,
+}
 
 
 def measured_peaks() -> dict:
@@ -351,7 +362,8 @@ def main():
     top_launch_ms = prof[top][1] / prof[top][0]
     achieved = abytes.get(top, 0) / (top_launch_ms / 1000.0) / 1e9
     roofline = {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peaks["hbm_gbs"],
-                "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": None,
+                "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
+                "traffic": NCU_DRAM_BYTES_C2.get(top) if args.config == "c2" else None,
                 "peak_source": peaks["source"], "launch_ms": top_launch_ms,
                 "algorithmic_bytes_per_launch": abytes.get(top, 0),
                 "share": {k: round(v / tot_ms, 4) for k, v in kernel_ms.items()}}
@@ -388,9 +400,12 @@ def main():
 
     extras = {}
     if not args.no_extras:
-        for name, kw in (("fast_f32", dict(fp_sum=2)),
-                         ("mixed_bf16", dict(storage=m.BF16, interp=m.INTERP_EXACT, fp_sum=2)),
-                         ("mixed_f16", dict(storage=m.F16, interp=m.INTERP_EXACT, fp_sum=2))):
+        # side measurements: the split-sum (Kahan) projector in FP32, and
+        # 16-bit storage of fields, projections and projector inputs with the
+        # reference-order projector and exact trilinear warps
+        for name, kw in (("split_kahan_f32", dict(fp_sum=2)),
+                         ("bf16_storage", dict(storage=m.BF16, interp=m.INTERP_EXACT)),
+                         ("f16_storage", dict(storage=m.F16, interp=m.INTERP_EXACT))):
             o = m.default_options(**kw)
             if o.storage == m.F32:
                 pr, Ft = proj, F0.clone()
