@@ -171,6 +171,12 @@ NCU_DRAM_BYTES_C2 = {
 }
 
 
+# Issue-slot utilisation (smsp__issue_active) of the projector and
+# backprojector from the same captures: these kernels are bound by issue and
+# latency, not by HBM.
+NCU_ISSUE_ACTIVE_C2 = {"fp_image": 0.417, "fp_motion": 0.429, "bp_div": 0.764}
+
+
 def measured_peaks() -> dict:
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -204,6 +210,39 @@ def cpu_threads() -> int:
         return len(os.sched_getaffinity(0))
     except AttributeError:
         return os.cpu_count() or 1
+
+
+def reference_gpu_step(p) -> dict:
+    """The reference's own CUDA code (host_AUMISART rebuilt from its unmodified
+    sources into oracle/_ref) timed on this GPU for one step of the same
+    workload: its host-pointer call, with its per-call allocations, copies and
+    device reset.  Reported beside the CPU arm, not as the arm's value."""
+    lib = os.path.join(ROOT, "oracle", "_ref", "libmcsart_ref.so")
+    if not os.path.exists(lib):
+        return {"unavailable": "the rebuilt reference library is not present"}
+    try:
+        import torch
+        if not torch.cuda.is_available():
+            return {"unavailable": "no CUDA device"}
+    except ImportError:
+        return {"unavailable": "torch is not importable"}
+    from oracle import ref_runner
+    ref = ref_runner.Ref()
+    g = p.geo
+    proj = np.stack([ref.projection(ref.deform(p.truth, float(p.volumes[v] - p.volumes[0]),
+                                               float(p.flows[v] - p.flows[0]), p.fields),
+                                    float(p.angles[v]), g) for v in range(p.cfg.n_views)])
+    it = {"n_iter": 2, "op_iter": np.array([1, 0], np.int32), "n_views": p.cfg.n_views,
+          "lambda": p.cfg.lam, "outIter": 1, "volumes": p.volumes, "flows": p.flows,
+          "angles": p.angles}
+    secs = []
+    for _ in range(3):  # the first call is a warm-up
+        r = ref_runner.aumisart(np.zeros_like(p.truth), proj, g, it, p.fields)
+        secs.append(float(r["seconds"]))
+    t = float(np.median(secs[1:]))
+    return {"value": 1.0 / t, "unit": "iterations/s", "seconds_per_step": t,
+            "kind": "reference CUDA build, host_AUMISART with host pointers",
+            "steps_timed": len(secs) - 1}
 
 
 def run_reference_arm(args, rank: int):
@@ -244,7 +283,8 @@ def run_reference_arm(args, rank: int):
             "e2e": {"value": value, "unit": "iterations/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0},
             "note": "the reference has no CPU implementation; this is the FP32 OpenMP "
-                    "transcription of its kernels and host_AUMISART loop"}
+                    "transcription of its kernels and host_AUMISART loop",
+            "reference_gpu": reference_gpu_step(p) if args.config == "c2" else None}
     print(json.dumps(line), flush=True)
 
 
@@ -364,6 +404,7 @@ def main():
     roofline = {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peaks["hbm_gbs"],
                 "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
                 "traffic": NCU_DRAM_BYTES_C2.get(top) if args.config == "c2" else None,
+                "issue_active_ncu": NCU_ISSUE_ACTIVE_C2 if args.config == "c2" else None,
                 "peak_source": peaks["source"], "launch_ms": top_launch_ms,
                 "algorithmic_bytes_per_launch": abytes.get(top, 0),
                 "share": {k: round(v / tot_ms, 4) for k, v in kernel_ms.items()}}
