@@ -284,7 +284,7 @@ def run_reference_arm(args, rank: int):
                     "d2h_bytes_per_step": 0},
             "note": "the reference has no CPU implementation; this is the FP32 OpenMP "
                     "transcription of its kernels and host_AUMISART loop",
-            "reference_gpu": reference_gpu_step(p) if args.config == "c2" else None}
+            "reference_gpu": reference_gpu_step(p)}
     print(json.dumps(line), flush=True)
 
 
@@ -472,6 +472,31 @@ def main():
             ext = max_over_ranks(e0.elapsed_time(e1) / 1000.0)
             extras[name] = {"value": args.steps / ext * world,
                             "unit": "iterations/s"}
+
+        # four independent problems of this workload (different seeds) run
+        # concurrently through mcsart_batch_run: problems per second x steps
+        nb_ = 4
+        batch = []
+        for s in range(nb_):
+            pb, prb, fb = build_problem(ctx, torch, args.config, seed=100 * (rank + 1) + s)
+            batch.append(dict(geo=pb.geo, n_views=nv, lambda_=pb.cfg.lam, angles=pb.angles,
+                              volumes=pb.volumes, flows=pb.flows,
+                              img=torch.zeros_like(img), proj=prb,
+                              fields=torch.stack(fb).contiguous() if fb else None))
+        for _ in range(2):
+            ctx.batch_run(batch, n_iter=2, op_iter=op, options=drop_in)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            ctx.batch_run(batch, n_iter=2, op_iter=op, options=drop_in)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ext = max_over_ranks(e0.elapsed_time(e1) / 1000.0)
+        extras["batch_4_problems"] = {
+            "value": nb_ * args.steps / ext * world, "unit": "iterations/s (all problems)",
+            "note": "4 independent problems of the workload, one mcsart_batch_run per step"}
+        del batch
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -193,6 +193,19 @@ typedef struct {
 int mcsart_aumisart_device(mcsart_ctx *ctx, const mcsart_problem *prob, int n_iter,
                            const int *h_op_iter, const mcsart_options *opt);
 
+/* Independent reconstructions run concurrently on one GPU.  No counterpart
+ * in the reference, which runs one problem per call (host_AUMISART,
+ * src/AUMISART.cu:143): one view's kernels leave most of a B200 idle, and
+ * problems of different sizes fill it together.  Each problem runs the same
+ * loop as mcsart_aumisart_device (same n_iter, op_iter and options for all)
+ * on a lane of its own (a stream, buffers and pass graphs kept by ctx, so
+ * repeated batches reuse them); results are bitwise those of separate
+ * mcsart_aumisart_device calls.  The lanes start after the work queued on
+ * ctx's stream, and ctx's stream waits for all of them. */
+#define MCSART_BATCH_MAX 64
+int mcsart_batch_run(mcsart_ctx *ctx, const mcsart_problem *problems, int n_problems,
+                     int n_iter, const int *h_op_iter, const mcsart_options *opt);
+
 /* ------------------------------------------ allocation-free projector */
 /* Largest volume, nx*ny*nz, that mcsart_projection_noalloc accepts: 2^22
  * voxels (e.g. 256x256x64), i.e. 16 MiB of FP32 scratch per device. */

@@ -76,6 +76,7 @@ SIGNATURES = {
     "mcsart_projection_views": [_P, _P, _P, _I, _F, _F, _F, _I, _F, _F, _I, _F, _I, _I, _I],
     "mcsart_aumisart": [_P] * 6 + [_I] * 8 + [_P] + [_F] * 8 + [_P] * 4 + [_P] * 6,
     "mcsart_aumisart_device": [ctypes.POINTER(Problem), _I, _P, ctypes.POINTER(Options)],
+    "mcsart_batch_run": [ctypes.POINTER(Problem), _I, _I, _P, ctypes.POINTER(Options)],
     "mcsart_set_stream": [_P],
     "mcsart_set_synchronous": [_I],
     "mcsart_set_interp": [_I],

@@ -78,6 +78,12 @@ struct mcsart_ctx {
     };
     std::map<std::string, Buf> ws;  // named device workspaces, grown on demand
     std::unique_ptr<mcsart::DriverState> driver;
+    // mcsart_batch_run: one lane (child context with its own stream, buffers
+    // and pass graphs) per concurrently running problem, and the events that
+    // order the lanes against this context's stream
+    std::vector<std::unique_ptr<mcsart_ctx>> lanes;
+    std::vector<cudaEvent_t> lane_done;
+    cudaEvent_t batch_start = nullptr;
     ~mcsart_ctx();
 };
 

@@ -182,6 +182,9 @@ static int prof_collect(mcsart_ctx *ctx) {
 }  // namespace mcsart
 
 mcsart_ctx::~mcsart_ctx() {
+    lanes.clear();
+    for (auto e : lane_done) cudaEventDestroy(e);
+    if (batch_start) cudaEventDestroy(batch_start);
     for (auto &r : prof_pending) {
         cudaEventDestroy(r.e0);
         cudaEventDestroy(r.e1);

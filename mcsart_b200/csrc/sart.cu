@@ -512,6 +512,56 @@ MC_EXPORT int mcsart_aumisart_device(mcsart_ctx *ctx, const mcsart_problem *prob
     return finish(ctx, "mcsart_aumisart_device");
 }
 
+MC_EXPORT int mcsart_batch_run(mcsart_ctx *ctx, const mcsart_problem *problems,
+                               int n_problems, int n_iter, const int *h_op_iter,
+                               const mcsart_options *opt) {
+    clear_error();
+    MC_TRY(validate_ctx(ctx));
+    MC_REQUIRE(problems != nullptr, "problems is NULL");
+    MC_REQUIRE(n_problems > 0 && n_problems <= MCSART_BATCH_MAX,
+               "n_problems must be in [1, %d] (got %d)", MCSART_BATCH_MAX, n_problems);
+    // lanes: child contexts on their own non-blocking streams
+    while ((int)ctx->lanes.size() < n_problems) {
+        std::unique_ptr<mcsart_ctx> lane(new mcsart_ctx());
+        lane->device = ctx->device;
+        MC_CHECK_CUDA(cudaStreamCreateWithFlags(&lane->own_stream, cudaStreamNonBlocking));
+        lane->stream = lane->own_stream;
+        cudaEvent_t done;
+        MC_CHECK_CUDA(cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
+        ctx->lane_done.push_back(done);
+        ctx->lanes.push_back(std::move(lane));
+    }
+    if (!ctx->batch_start)
+        MC_CHECK_CUDA(cudaEventCreateWithFlags(&ctx->batch_start, cudaEventDisableTiming));
+    // the lanes start after the work already queued on the caller's stream
+    MC_CHECK_CUDA(cudaEventRecord(ctx->batch_start, ctx->stream));
+    int rc = MCSART_OK, started = 0;
+    char msg[512] = "";
+    for (int i = 0; i < n_problems; i++) {
+        mcsart_ctx *lane = ctx->lanes[i].get();
+        lane->profiling = ctx->profiling;
+        MC_CHECK_CUDA(cudaStreamWaitEvent(lane->stream, ctx->batch_start, 0));
+        const long long l0 = lane->launches;
+        started = i + 1;
+        rc = mcsart_aumisart_device(lane, &problems[i], n_iter, h_op_iter, opt);
+        ctx->launches += lane->launches - l0;
+        if (rc != MCSART_OK) {
+            snprintf(msg, sizeof(msg), "problem %d: %s", i, mcsart_last_error());
+            break;
+        }
+    }
+    // the caller's stream waits for every lane that was started, also on error
+    for (int i = 0; i < started; i++) {
+        MC_CHECK_CUDA(cudaEventRecord(ctx->lane_done[i], ctx->lanes[i]->stream));
+        MC_CHECK_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->lane_done[i], 0));
+    }
+    if (rc != MCSART_OK) {
+        set_error("%s", msg);
+        return rc;
+    }
+    return finish(ctx, "mcsart_batch_run");
+}
+
 MC_EXPORT int mcsart_aumisart(mcsart_ctx *ctx, float *h_outimg, float *h_outproj,
                               float *h_outnorm, float *h_outalphax, const float *h_img,
                               const float *h_proj, int nx, int ny, int nz, int na, int nb,

@@ -250,6 +250,25 @@ class Context:
                    h(err_weights, name="err_weights") if err_weights is not None else None,
                    h(angles, name="angles"), *[h(f, name="field") for f in (ax, ay, az, bx, by, bz)])
 
+    @staticmethod
+    def _problem(geo, n_views, lambda_, angles, volumes, flows, img, proj, fields, resid, norm,
+                 options):
+        """A Problem struct and the host arrays it points into (keep them alive)."""
+        es = 4 if options is None or options.storage == F32 else 2
+        p = Problem()
+        p.nx, p.ny, p.nz = int(geo["nx"]), int(geo["ny"]), int(geo["nz"])
+        p.na, p.nb, p.n_views = int(geo["na"]), int(geo["nb"]), int(n_views)
+        p.SO, p.SD, p.da, p.db = geo["SO"], geo["SD"], geo["da"], geo["db"]
+        p.ai, p.bi, p.lambda_ = geo["ai"], geo["bi"], float(lambda_)
+        keep = [np.ascontiguousarray(x, dtype=np.float32) for x in (angles, volumes, flows)]
+        p.h_angles, p.h_volumes, p.h_flows = [_hptr(x) for x in keep]
+        p.d_img = _ptr(img, "img", 4)
+        p.d_proj = _ptr(proj, "proj", es)
+        p.d_fields = _ptr(fields, "fields", es)
+        p.d_resid = _ptr(resid, "resid", 4)
+        p.d_norm = _ptr(norm, "norm", 4)
+        return p, keep
+
     def aumisart_device(self, *, geo, n_views, lambda_, angles, volumes, flows, img, proj,
                         fields=None, resid=None, norm=None, n_iter, op_iter, options=None):
         """Device-resident driver (mcsart_aumisart_device).
@@ -257,19 +276,28 @@ class Context:
         img: float32 CUDA tensor (updated in place); proj, fields: CUDA tensors of
         the options' storage type; resid/norm: optional float32 outputs.
         """
-        es = 4 if options is None or options.storage == F32 else 2
-        p = Problem()
-        p.nx, p.ny, p.nz = int(geo["nx"]), int(geo["ny"]), int(geo["nz"])
-        p.na, p.nb, p.n_views = int(geo["na"]), int(geo["nb"]), int(n_views)
-        p.SO, p.SD, p.da, p.db = geo["SO"], geo["SD"], geo["da"], geo["db"]
-        p.ai, p.bi, p.lambda_ = geo["ai"], geo["bi"], float(lambda_)
-        self._keep = [np.ascontiguousarray(x, dtype=np.float32) for x in (angles, volumes, flows)]
-        p.h_angles, p.h_volumes, p.h_flows = [_hptr(x) for x in self._keep]
-        p.d_img = _ptr(img, "img", 4)
-        p.d_proj = _ptr(proj, "proj", es)
-        p.d_fields = _ptr(fields, "fields", es)
-        p.d_resid = _ptr(resid, "resid", 4)
-        p.d_norm = _ptr(norm, "norm", 4)
+        p, self._keep = self._problem(geo, n_views, lambda_, angles, volumes, flows, img, proj,
+                                      fields, resid, norm, options)
         op = np.ascontiguousarray(op_iter, dtype=np.int32)
         self._call("mcsart_aumisart_device", ctypes.byref(p), int(n_iter), _hptr(op),
+                   ctypes.byref(options) if options is not None else None)
+
+    def batch_run(self, problems, *, n_iter, op_iter, options=None):
+        """Independent reconstructions run concurrently (mcsart_batch_run).
+
+        problems: list of dicts with the keyword arguments of aumisart_device
+        (geo, n_views, lambda_, angles, volumes, flows, img, proj and optionally
+        fields, resid, norm); every problem runs n_iter iterations of op_iter.
+        """
+        structs, keep = [], []
+        for q in problems:
+            p, k = self._problem(q["geo"], q["n_views"], q["lambda_"], q["angles"], q["volumes"],
+                                 q["flows"], q["img"], q["proj"], q.get("fields"), q.get("resid"),
+                                 q.get("norm"), options)
+            structs.append(p)
+            keep.append(k)
+        arr = (Problem * len(structs))(*structs)
+        self._keep = keep
+        op = np.ascontiguousarray(op_iter, dtype=np.int32)
+        self._call("mcsart_batch_run", arr, len(structs), int(n_iter), _hptr(op),
                    ctypes.byref(options) if options is not None else None)
