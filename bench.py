@@ -441,12 +441,18 @@ def main():
 
     extras = {}
     if not args.no_extras:
-        # side measurements: the split-sum (Kahan) projector in FP32, and
-        # 16-bit storage of fields, projections and projector inputs with the
-        # reference-order projector and exact trilinear warps
+        # side measurements: the split-sum (Kahan) projector in FP32, 16-bit
+        # storage of fields, projections and projector inputs with the
+        # reference-order projector and exact trilinear warps, and ordered
+        # subsets
         for name, kw in (("split_kahan_f32", dict(fp_sum=2)),
                          ("bf16_storage", dict(storage=m.BF16, interp=m.INTERP_EXACT)),
-                         ("f16_storage", dict(storage=m.F16, interp=m.INTERP_EXACT))):
+                         ("f16_storage", dict(storage=m.F16, interp=m.INTERP_EXACT)),
+                         # ordered subsets of 8 views (a different algorithm:
+                         # one projector and one backprojector launch per subset)
+                         ("subsets_of_8_f32", dict(subset=8)),
+                         ("subsets_of_8_bf16", dict(subset=8, storage=m.BF16,
+                                                    interp=m.INTERP_EXACT))):
             o = m.default_options(**kw)
             if o.storage == m.F32:
                 pr, Ft = proj, F0.clone()

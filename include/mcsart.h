@@ -171,6 +171,12 @@ typedef struct {
                          ray (bitwise drop-in); 1 = per-slab partial sums, slabs split
                          across warps; 2 = as 1 with Kahan-compensated slab sums */
     int fp_groups;    /* slab groups per ray in modes 1 and 2 (0 = auto) */
+    int subset;       /* image passes: views per ordered subset, 1..16 (0 = 1).  1 is
+                         the reference's view-by-view loop.  k > 1: the k views of a
+                         subset each compute the reference's correction from the same
+                         image, in one projector and one backprojector launch, and the
+                         image receives lambda/k times their sum (a different
+                         algorithm from the reference's, not a drop-in) */
 } mcsart_options;
 void mcsart_default_options(mcsart_options *opt);
 
@@ -192,6 +198,23 @@ typedef struct {
  * of host_AUMISART's loop on device-resident buffers. */
 int mcsart_aumisart_device(mcsart_ctx *ctx, const mcsart_problem *prob, int n_iter,
                            const int *h_op_iter, const mcsart_options *opt);
+
+/* As mcsart_aumisart, returning all six final DVF fields (h_out_ax is
+ * required, the other five may be NULL).  The reference returns alpha_x only
+ * (src/AUMISART.cu:291).  The loop keeps no state between iterations other
+ * than the image and the six fields, so passing the returned image and fields
+ * back as inputs continues a reconstruction exactly where it stopped: n + m
+ * iterations in two calls give the bits of one call of n + m iterations. */
+int mcsart_aumisart_fields(mcsart_ctx *ctx, float *h_outimg, float *h_outproj, float *h_outnorm,
+                           float *h_out_ax, float *h_out_ay, float *h_out_az, float *h_out_bx,
+                           float *h_out_by, float *h_out_bz, const float *h_img,
+                           const float *h_proj, int nx, int ny, int nz, int na, int nb,
+                           int outIter, int n_views, int n_iter, const int *op_iter, float da,
+                           float db, float ai, float bi, float SO, float SD, float dx,
+                           float lambda, const float *volumes, const float *flows,
+                           const float *err_weights, const float *angles, const float *alpha_x,
+                           const float *alpha_y, const float *alpha_z, const float *beta_x,
+                           const float *beta_y, const float *beta_z);
 
 /* Independent reconstructions run concurrently on one GPU.  No counterpart
  * in the reference, which runs one problem per call (host_AUMISART,

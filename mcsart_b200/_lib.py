@@ -35,7 +35,7 @@ class McsartError(RuntimeError):
 
 class Options(ctypes.Structure):
     _fields_ = [("storage", ctypes.c_int), ("interp", ctypes.c_int), ("use_graph", ctypes.c_int),
-                ("fp_sum", ctypes.c_int), ("fp_groups", ctypes.c_int)]
+                ("fp_sum", ctypes.c_int), ("fp_groups", ctypes.c_int), ("subset", ctypes.c_int)]
 
 
 class Problem(ctypes.Structure):
@@ -75,6 +75,7 @@ SIGNATURES = {
     "mcsart_snrm2": [_I, _P, ctypes.POINTER(ctypes.c_float)],
     "mcsart_projection_views": [_P, _P, _P, _I, _F, _F, _F, _I, _F, _F, _I, _F, _I, _I, _I],
     "mcsart_aumisart": [_P] * 6 + [_I] * 8 + [_P] + [_F] * 8 + [_P] * 4 + [_P] * 6,
+    "mcsart_aumisart_fields": [_P] * 11 + [_I] * 8 + [_P] + [_F] * 8 + [_P] * 4 + [_P] * 6,
     "mcsart_aumisart_device": [ctypes.POINTER(Problem), _I, _P, ctypes.POINTER(Options)],
     "mcsart_batch_run": [ctypes.POINTER(Problem), _I, _I, _P, ctypes.POINTER(Options)],
     "mcsart_set_stream": [_P],

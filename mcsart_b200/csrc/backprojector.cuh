@@ -87,7 +87,16 @@ struct BPArgs {
                           // volume updated in place
     float *outT;          // BP_DIV_ADD: y-fastest copy refreshed alongside (nullable)
     cudaSurfaceObject_t outSurf;  // BP_DIV: 3D array receiving the ratio (0 = none)
+    // Several views per launch (K == 2): n_views views of an ordered subset,
+    // angles[v] (device) and pair + v*na*nb.  BP_DIV writes view v's ratio to
+    // out + v*V and outSurfs[v]; BP_DIV_ADD adds lambda times the sum of the
+    // views' ratios (summed in view order) to out.  n_views <= 1 with
+    // angles == nullptr is the single view at `angle`.
+    int n_views;
+    const float *angles;
+    cudaSurfaceObject_t outSurfs[16];
 };
+constexpr int BP_MAX_VIEWS = 16;
 
 // Voxel columns per block: 32 (x) by BP_ROWS (y), BP_NZ slices per thread.
 #ifndef MCSART_BP_NZ
@@ -102,12 +111,90 @@ constexpr int BP_NZ = MCSART_BP_NZ;
 // detector rows take the general loop.
 constexpr int BP_WB = 4;
 
+// Overlap-weighted gather of one view for the BP_NZ voxels (ix, iy, z0 ..)
+// of a thread: acc0 (and acc1 with K == 2) get the view's terms in the
+// reference's order (detector column outer, row inner, acc = fma(wa*wb, p,
+// acc), :150-168).  The column box and the column weights wa are shared by the
+// voxels of a thread, the row weights wb are computed once per voxel.
+template <int K>
+__device__ __forceinline__ void bp_gather_view(const BPArgs &p, float angle, const float *proj,
+                                               const float2 *pair, int ix, int iy, int z0,
+                                               float *acc0, float *acc1) {
+    const Geom &g = p.g;
+    const int na = g.na;
+    const float sphi = __sinf(angle), cphi = __cosf(angle);
+    const BPColumn col = bp_column(ix, iy, cphi, sphi, g);
+    // rows of each slice: first row, count (BP_WB + 1 = more than BP_WB),
+    // row weights, box
+    int ib0[BP_NZ], nbk[BP_NZ];
+    float wb[BP_NZ][BP_WB], bmn[BP_NZ], bmx[BP_NZ];
+#pragma unroll
+    for (int k = 0; k < BP_NZ; k++) {
+        nbk[k] = 0;
+        ib0[k] = 0;
+        bmn[k] = 0.0f;
+        bmx[k] = 0.0f;
+#pragma unroll
+        for (int j = 0; j < BP_WB; j++) wb[k][j] = 0.0f;
+        const int iz = z0 + k;
+        if (iz < g.nz) {
+            bp_rows(col, iz, g, bmn[k], bmx[k]);
+            const float blim = ((float)g.nb < bmx[k]) ? (float)g.nb : bmx[k];  // MIN(nb, b_max)
+            ib0[k] = max(0, (int)floorf(fmaxf(bmn[k], -1.0f)));
+            // rows ib >= ib0 with (float)ib < blim, i.e. ib < ceil(blim)
+            // (blim <= nb, so every row index is exact in float; a NaN
+            // converts to 0 and gives no rows, as the loop test would)
+            nbk[k] = min(BP_WB + 1, max(0, (int)ceilf(blim) - ib0[k]));
+#pragma unroll
+            for (int j = 0; j < BP_WB; j++) {
+                const int ib = ib0[k] + j;
+                wb[k][j] = fminf(ib + 1.0f, bmx[k]) - fmaxf(ib + 0.0f, bmn[k]);
+            }
+        }
+    }
+    const float alim = ((float)na < col.amax) ? (float)na : col.amax;  // MIN(na, a_max)
+    const int ia0 = max(0, (int)floorf(fmaxf(col.amin, -1.0f)));
+    for (int ia = ia0; (float)ia < alim; ia++) {
+        const float wa = fminf(ia + 1.0f, col.amax) - fmaxf(ia + 0.0f, col.amin);
+#pragma unroll
+        for (int k = 0; k < BP_NZ; k++) {
+            if (nbk[k] <= BP_WB) {
+#pragma unroll
+                for (int j = 0; j < BP_WB; j++) {
+                    if (j < nbk[k]) {
+                        const float w = __fmul_rn(wa, wb[k][j]);
+                        const int pix = ia + (ib0[k] + j) * na;
+                        if (K == 1) {
+                            acc0[k] = __fmaf_rn(w, __ldg(proj + pix), acc0[k]);
+                        } else {
+                            const float2 v = __ldg(pair + pix);
+                            acc0[k] = __fmaf_rn(w, v.x, acc0[k]);
+                            acc1[k] = __fmaf_rn(w, v.y, acc1[k]);
+                        }
+                    }
+                }
+            } else {
+                const float blim = ((float)g.nb < bmx[k]) ? (float)g.nb : bmx[k];
+                for (int ib = ib0[k]; (float)ib < blim; ib++) {
+                    const float w =
+                        __fmul_rn(wa, fminf(ib + 1.0f, bmx[k]) - fmaxf(ib + 0.0f, bmn[k]));
+                    const int pix = ia + ib * na;
+                    if (K == 1) {
+                        acc0[k] = __fmaf_rn(w, __ldg(proj + pix), acc0[k]);
+                    } else {
+                        const float2 v = __ldg(pair + pix);
+                        acc0[k] = __fmaf_rn(w, v.x, acc0[k]);
+                        acc1[k] = __fmaf_rn(w, v.y, acc1[k]);
+                    }
+                }
+            }
+        }
+    }
+}
+
 // blockDim = (32, BP_ROWS); each thread backprojects the BP_NZ voxels
-// (ix, iy, z0 .. z0 + BP_NZ - 1), z0 = blockIdx.z * BP_NZ.  Per voxel the
-// terms are accumulated in the reference's order (detector column outer,
-// row inner, acc = fma(wa*wb, p, acc), :150-168); the column box and the
-// column weights wa are shared by the voxels of a thread, the row weights wb
-// are computed once per voxel instead of once per (column, row).
+// (ix, iy, z0 .. z0 + BP_NZ - 1), z0 = blockIdx.z * BP_NZ, for every view of
+// the launch.
 template <int K, int MODE>
 __global__ void __launch_bounds__(256, MCSART_BP_MINBLOCKS) bp_kernel(const BPArgs p) {
     __shared__ float tile[BP_NZ][BP_ROWS][33];
@@ -116,111 +203,51 @@ __global__ void __launch_bounds__(256, MCSART_BP_MINBLOCKS) bp_kernel(const BPAr
     const int x0 = blockIdx.x * 32, y0 = blockIdx.y * BP_ROWS, z0 = blockIdx.z * BP_NZ;
     const int ix = x0 + tx, iy = y0 + ty;
     const bool active = ix < g.nx && iy < g.ny;
-    const float sphi = __sinf(p.angle), cphi = __cosf(p.angle);
-    const int na = g.na;
+    const int64_t plane = (int64_t)g.nx * g.ny, V = plane * g.nz, NP = (int64_t)g.na * g.nb;
+    const int nv = (K == 2 && p.n_views > 1) ? p.n_views : 1;
 
-    float acc0[BP_NZ], acc1[BP_NZ];
+    float qsum[BP_NZ];
 #pragma unroll
-    for (int k = 0; k < BP_NZ; k++) { acc0[k] = 0.0f; acc1[k] = 0.0f; }
-
-    if (active) {
-        const BPColumn col = bp_column(ix, iy, cphi, sphi, g);
-        // rows of each slice: first row, count (BP_WB + 1 = more than BP_WB),
-        // row weights, box
-        int ib0[BP_NZ], nbk[BP_NZ];
-        float wb[BP_NZ][BP_WB], bmn[BP_NZ], bmx[BP_NZ];
+    for (int k = 0; k < BP_NZ; k++) qsum[k] = 0.0f;
+    for (int v = 0; v < nv; v++) {
+        float acc0[BP_NZ], acc1[BP_NZ];
+#pragma unroll
+        for (int k = 0; k < BP_NZ; k++) { acc0[k] = 0.0f; acc1[k] = 0.0f; }
+        const float angle = p.angles ? p.angles[v] : p.angle;
+        if (active) bp_gather_view<K>(p, angle, p.proj, p.pair + v * NP, ix, iy, z0, acc0, acc1);
 #pragma unroll
         for (int k = 0; k < BP_NZ; k++) {
-            nbk[k] = 0;
-            ib0[k] = 0;
-            bmn[k] = 0.0f;
-            bmx[k] = 0.0f;
-#pragma unroll
-            for (int j = 0; j < BP_WB; j++) wb[k][j] = 0.0f;
             const int iz = z0 + k;
-            if (iz < g.nz) {
-                bp_rows(col, iz, g, bmn[k], bmx[k]);
-                const float blim = ((float)g.nb < bmx[k]) ? (float)g.nb : bmx[k];  // MIN(nb, b_max)
-                ib0[k] = max(0, (int)floorf(fmaxf(bmn[k], -1.0f)));
-                // rows ib >= ib0 with (float)ib < blim, i.e. ib < ceil(blim)
-                // (blim <= nb, so every row index is exact in float; a NaN
-                // converts to 0 and gives no rows, as the loop test would)
-                nbk[k] = min(BP_WB + 1, max(0, (int)ceilf(blim) - ib0[k]));
-#pragma unroll
-                for (int j = 0; j < BP_WB; j++) {
-                    const int ib = ib0[k] + j;
-                    wb[k][j] = fminf(ib + 1.0f, bmx[k]) - fmaxf(ib + 0.0f, bmn[k]);
-                }
+            if (!(active && iz < g.nz)) continue;
+            const int64_t id = ix + (int64_t)iy * g.nx + iz * plane;
+            if (MODE == BP_PLAIN) {
+                p.out[id] = acc0[k];
+                continue;
             }
-        }
-        const float alim = ((float)na < col.amax) ? (float)na : col.amax;  // MIN(na, a_max)
-        const int ia0 = max(0, (int)floorf(fmaxf(col.amin, -1.0f)));
-        for (int ia = ia0; (float)ia < alim; ia++) {
-            const float wa = fminf(ia + 1.0f, col.amax) - fmaxf(ia + 0.0f, col.amin);
-#pragma unroll
-            for (int k = 0; k < BP_NZ; k++) {
-                if (nbk[k] <= BP_WB) {
-#pragma unroll
-                    for (int j = 0; j < BP_WB; j++) {
-                        if (j < nbk[k]) {
-                            const float w = __fmul_rn(wa, wb[k][j]);
-                            const int pix = ia + (ib0[k] + j) * na;
-                            if (K == 1) {
-                                acc0[k] = __fmaf_rn(w, __ldg(p.proj + pix), acc0[k]);
-                            } else {
-                                const float2 v = __ldg(p.pair + pix);
-                                acc0[k] = __fmaf_rn(w, v.x, acc0[k]);
-                                acc1[k] = __fmaf_rn(w, v.y, acc1[k]);
-                            }
-                        }
-                    }
-                } else {
-                    const float blim = ((float)g.nb < bmx[k]) ? (float)g.nb : bmx[k];
-                    for (int ib = ib0[k]; (float)ib < blim; ib++) {
-                        const float w =
-                            __fmul_rn(wa, fminf(ib + 1.0f, bmx[k]) - fmaxf(ib + 0.0f, bmn[k]));
-                        const int pix = ia + ib * na;
-                        if (K == 1) {
-                            acc0[k] = __fmaf_rn(w, __ldg(p.proj + pix), acc0[k]);
-                        } else {
-                            const float2 v = __ldg(p.pair + pix);
-                            acc0[k] = __fmaf_rn(w, v.x, acc0[k]);
-                            acc1[k] = __fmaf_rn(w, v.y, acc1[k]);
-                        }
-                    }
-                }
+            float q = acc0[k] / acc1[k];            // cu_division.cu:20
+            if (isnan(q) || isinf(q)) q = 0.0f;     // :21-24
+            if (MODE == BP_DIV) {
+                if (p.out) p.out[id + v * V] = q;
+                const cudaSurfaceObject_t s = nv > 1 ? p.outSurfs[v] : p.outSurf;
+                if (s) surf3Dwrite(q, s, ix * (int)sizeof(float), iy, iz, cudaBoundaryModeZero);
+            } else {
+                qsum[k] = v == 0 ? q : qsum[k] + q;  // subset: ratios summed in view order
             }
         }
     }
-
-    const int64_t plane = (int64_t)g.nx * g.ny;
+    if (MODE != BP_DIV_ADD) return;
 #pragma unroll
     for (int k = 0; k < BP_NZ; k++) {
         const int iz = z0 + k;
         float val = 0.0f;
         if (active && iz < g.nz) {
             const int64_t id = ix + (int64_t)iy * g.nx + iz * plane;
-            if (MODE == BP_PLAIN) {
-                val = acc0[k];
-                p.out[id] = val;
-            } else {
-                float q = acc0[k] / acc1[k];            // cu_division.cu:20
-                if (isnan(q) || isinf(q)) q = 0.0f;     // :21-24
-                if (MODE == BP_DIV) {
-                    val = q;
-                    if (p.out) p.out[id] = val;
-                    if (p.outSurf)
-                        surf3Dwrite(val, p.outSurf, ix * (int)sizeof(float), iy, iz,
-                                    cudaBoundaryModeZero);
-                } else {
-                    val = __fmaf_rn(q, p.lambda, p.out[id]);  // cu_add.cu:17
-                    p.out[id] = val;
-                }
-            }
+            val = __fmaf_rn(qsum[k], p.lambda, p.out[id]);  // cu_add.cu:17
+            p.out[id] = val;
         }
-        if (MODE == BP_DIV_ADD) tile[k][ty][tx] = val;
+        tile[k][ty][tx] = val;
     }
-    if (MODE == BP_DIV_ADD && p.outT != nullptr) {
+    if (p.outT != nullptr) {
         __syncthreads();
         // transposed store outT[iy + ix*ny + iz*nx*ny]: 8 consecutive iy per ix
         const int t = ty * 32 + tx;

@@ -244,6 +244,11 @@ template <typename VT, int K, typename MT = VT> struct FPArgs {
     float *resid;       // residual output (nullable)
     float2 *bp_in;      // (residual, ones-projection) pairs for the backprojector
     double2 *norm_part; // per-block (sum b^2, sum r^2)
+    // several views per launch (fp_ref_kernel, view = blockIdx.z): meas,
+    // resid and bp_in advance by na*nb per view, norm_part by the blocks of
+    // one view, and the volumes by vol_stride elements per view (0: every
+    // view projects the same volumes)
+    int64_t vol_stride;
 };
 
 // ------------------------------------------------------------------------
@@ -433,19 +438,20 @@ __global__ void __launch_bounds__(FPC_THREADS, FPC_MIN_BLOCKS) fp_ref_kernel(con
     const VT *base[K];
     int su, sd;
     const int sz = g.nx * g.ny;
+    const int64_t voff = (int64_t)blockIdx.z * p.vol_stride;
     if (r.xdrive) {
         if (p.vol.tr[0] != nullptr) {
 #pragma unroll
-            for (int k = 0; k < K; k++) base[k] = p.vol.tr[k];
+            for (int k = 0; k < K; k++) base[k] = p.vol.tr[k] + voff;
             su = 1; sd = g.ny;
         } else {
 #pragma unroll
-            for (int k = 0; k < K; k++) base[k] = p.vol.std[k];
+            for (int k = 0; k < K; k++) base[k] = p.vol.std[k] + voff;
             su = g.nx; sd = 1;
         }
     } else {
 #pragma unroll
-        for (int k = 0; k < K; k++) base[k] = p.vol.std[k];
+        for (int k = 0; k < K; k++) base[k] = p.vol.std[k] + voff;
         su = 1; sd = g.nx;
     }
     const float z_half = (float)(g.nz / 2);
@@ -538,12 +544,13 @@ __global__ void __launch_bounds__(FPC_THREADS, FPC_MIN_BLOCKS) fp_ref_kernel(con
     }
 
     const int64_t pix = ia + (int64_t)ib * g.na;
+    const int64_t vpix = pix + (int64_t)blockIdx.z * g.na * g.nb;  // this view's cell
     double nb2 = 0.0, nr2 = 0.0;
     if (active) {
         if (p.mode == FP_PLAIN) {
-            p.out[pix + (int64_t)blockIdx.z * g.na * g.nb] = acc[0];
+            p.out[vpix] = acc[0];
         } else {
-            const float b = ldv(p.meas, pix);
+            const float b = ldv(p.meas, vpix);
             // AUMISART.cu:206 host_add(proj, proj_temp, -1): proj += proj_temp * -1
             float res = __fmaf_rn(acc[0], -1.0f, b);
             float ones = ONES ? accw : 0.0f;
@@ -551,8 +558,8 @@ __global__ void __launch_bounds__(FPC_THREADS, FPC_MIN_BLOCKS) fp_ref_kernel(con
                 res = __fmaf_rn(acc[K > 1 ? 1 : 0], 1.0f, res);  // AUMISART.cu:260, + FP(img0)
                 if (K >= 3) ones = acc[K - 1];                   // FP(initial2(...)), :267-268
             }
-            if (p.resid) p.resid[pix] = res;
-            p.bp_in[pix] = make_float2(res, ones);
+            if (p.resid) p.resid[vpix] = res;
+            p.bp_in[vpix] = make_float2(res, ones);
             nb2 = (double)b * (double)b;
             nr2 = (double)res * (double)res;
         }
@@ -572,7 +579,8 @@ __global__ void __launch_bounds__(FPC_THREADS, FPC_MIN_BLOCKS) fp_ref_kernel(con
             tb += sm_norm[w].x;
             tr += sm_norm[w].y;
         }
-        p.norm_part[blockIdx.y * gridDim.x + blockIdx.x] = make_double2(tb, tr);
+        p.norm_part[(int64_t)blockIdx.z * gridDim.x * gridDim.y + blockIdx.y * gridDim.x +
+                    blockIdx.x] = make_double2(tb, tr);
     }
 }
 

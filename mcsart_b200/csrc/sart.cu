@@ -82,6 +82,7 @@ template <typename ST, int INTERP, int SUM> struct Runner {
     const mcsart_options &opt;
     int64_t V = 0, NP = 0;
     int fp_bx = 0, fp_by = 0, fp_blocks = 0, groups = 1;
+    int subset = 1;  // views per ordered subset in image passes
     std::vector<int> views_img, views_mot;
 
     Runner(mcsart_ctx *c, const Problem &p, const mcsart_options &o)
@@ -94,6 +95,7 @@ template <typename ST, int INTERP, int SUM> struct Runner {
         groups = SUM == SUM_REF ? 1
                  : opt.fp_groups > 0 ? std::min(opt.fp_groups, 8)
                                      : fp_auto_groups(fp_blocks, std::max(P.g.nx, P.g.ny));
+        subset = std::min(std::max(opt.subset, 1), BP_MAX_VIEWS);
         for (int v = 0; v < P.n_views; v++) views_img.push_back(v);
         const int step = P.motion_model ? 1 : 10;  // AUMISART.cu:242 vs :72
         for (int v = 1; v < P.n_views; v += step) views_mot.push_back(v);
@@ -107,21 +109,26 @@ template <typename ST, int INTERP, int SUM> struct Runner {
 
     int alloc() {
         const size_t vs = V * sizeof(ST), vf = V * sizeof(float);
-        MC_TRY(S.img1.ensure(vs));
-        MC_TRY(S.img1T.ensure(vs));
+        MC_TRY(S.img1.ensure(vs * subset));
+        MC_TRY(S.img1T.ensure(vs * subset));
         MC_TRY(S.imgS.ensure(vs));
         MC_TRY(S.imgST.ensure(vs));
         MC_TRY(S.img0.ensure(vs));
         MC_TRY(S.img0T.ensure(vs));
         MC_TRY(S.ones.ensure(vs));
         MC_TRY(S.onesT.ensure(vs));
-        MC_TRY(S.ratio.ensure(vf));
+        MC_TRY(S.ratio.ensure(vf * subset));
         MC_TRY(S.imgT.ensure(vf));
-        MC_TRY(S.pairs.ensure(NP * sizeof(float2)));
+        MC_TRY(S.pairs.ensure(NP * subset * sizeof(float2)));
         if (INTERP == MCSART_INTERP_TEXTURE && P.motion_model) {
             MC_TRY(S.tv_img.ensure(P.g.nx, P.g.ny, P.g.nz));
             MC_TRY(S.tv_ratio.ensure(P.g.nx, P.g.ny, P.g.nz));
+            for (int j = 1; j < subset; j++)
+                MC_TRY(S.tv_ratio_sub[j - 1].ensure(P.g.nx, P.g.ny, P.g.nz));
         }
+        MC_TRY(S.angles_dev.ensure((size_t)P.n_views * sizeof(float)));
+        MC_CHECK_CUDA(cudaMemcpyAsync(S.angles_dev.ptr, P.angles, P.n_views * sizeof(float),
+                                      cudaMemcpyHostToDevice, ctx->stream));
         MC_TRY(S.norm_part.ensure((size_t)P.n_views * fp_blocks * sizeof(double2)));
         MC_TRY(S.norm_tmp.ensure((size_t)P.n_views * sizeof(float)));
         MC_TRY(S.views_image.ensure((size_t)P.n_views * sizeof(int)));
@@ -182,6 +189,56 @@ template <typename ST, int INTERP, int SUM> struct Runner {
         return MCSART_OK;
     }
 
+    // Ordered subset of kk > 1 views v0 .. v0+kk-1 (list positions k0 ..): one
+    // projector launch over the kk views (view = blockIdx.z), the volumes of
+    // view j at +j*vol_stride.
+    template <int K, bool ONES, typename VT>
+    int launch_fp_subset(const FPVolumes<VT, K> &vol, int v0, int k0, int kk, int mode,
+                         int64_t vol_stride) {
+        FPArgs<VT, K, ST> a{};
+        a.vol = vol;
+        a.g = P.g;
+        a.angle = P.angles[v0];
+        a.angles = S.angles_dev.as<float>() + v0;
+        a.mode = mode;
+        a.meas = meas(v0);
+        a.resid = (mode == FP_IMAGE && P.resid) ? P.resid + (int64_t)v0 * NP : nullptr;
+        a.bp_in = S.pairs.as<float2>();
+        a.norm_part = S.norm_part.as<double2>() + (int64_t)k0 * fp_blocks;
+        a.vol_stride = vol_stride;
+        ctx->label = mode == FP_MOTION ? "fp_motion" : "fp_image";
+        MC_LAUNCH(ctx, (fp_ref_kernel<K, ONES, VT, ST>), dim3(fp_bx, fp_by, kk), dim3(FPC_THREADS),
+                  0, a);
+        return MCSART_OK;
+    }
+
+    // One backprojector launch over the subset: BP_DIV writes view j's ratio
+    // to out + j*V / surfs[j]; BP_DIV_ADD adds lambda/kk times the sum of the
+    // views' ratios to out.
+    int launch_bp_subset(int v0, int kk, int mode, float *out, float *outT,
+                         const cudaSurfaceObject_t *surfs) {
+        BPArgs b{};
+        b.pair = S.pairs.as<float2>();
+        b.g = P.g;
+        b.angle = P.angles[v0];
+        b.angles = S.angles_dev.as<float>() + v0;
+        b.n_views = kk;
+        b.lambda = P.lambda / (float)kk;
+        b.out = out;
+        b.outT = outT;
+        for (int j = 0; j < kk && surfs; j++) b.outSurfs[j] = surfs[j];
+        const dim3 grid(div_up(P.g.nx, 32), div_up(P.g.ny, BP_ROWS), div_up(P.g.nz, BP_NZ)),
+            block(32, BP_ROWS);
+        if (mode == BP_DIV) {
+            ctx->label = "bp_div";
+            MC_LAUNCH(ctx, (bp_kernel<2, BP_DIV>), grid, block, 0, b);
+        } else {
+            ctx->label = "bp_div_add";
+            MC_LAUNCH(ctx, (bp_kernel<2, BP_DIV_ADD>), grid, block, 0, b);
+        }
+        return MCSART_OK;
+    }
+
     dim3 tile_grid() const { return dim3(div_up(P.g.nx, 32), div_up(P.g.ny, 32), P.g.nz); }
 
     int finalize_norms(const int *views_dev, int n) {
@@ -200,12 +257,72 @@ template <typename ST, int INTERP, int SUM> struct Runner {
         FPVolumes<float, 1> vol{};
         vol.std[0] = P.img;
         vol.tr[0] = S.imgT.as<float>();
-        for (int k = 0; k < (int)views_img.size(); k++) {
-            const int v = views_img[k];
-            MC_TRY((launch_fp<1, true, float>(vol, v, k, FP_IMAGE)));
-            MC_TRY(launch_bp(v, BP_DIV_ADD, P.img, S.imgT.as<float>()));
+        const int n = (int)views_img.size();
+        for (int k = 0; k < n; k += subset) {
+            const int kk = std::min(subset, n - k), v = views_img[k];
+            if (kk == 1) {  // one view at a time: the reference's loop
+                MC_TRY((launch_fp<1, true, float>(vol, v, k, FP_IMAGE)));
+                MC_TRY(launch_bp(v, BP_DIV_ADD, P.img, S.imgT.as<float>()));
+            } else {
+                MC_TRY((launch_fp_subset<1, true, float>(vol, v, k, kk, FP_IMAGE, 0)));
+                MC_TRY(launch_bp_subset(v, kk, BP_DIV_ADD, P.img, S.imgT.as<float>(), nullptr));
+            }
         }
         return finalize_norms(S.views_image.as<int>(), (int)views_img.size());
+    }
+
+    // Ordered subset of kk > 1 views in the motion-compensated image pass:
+    // every view warps the same image to its phase (:193), one projector
+    // launch and one backprojector launch serve the kk views, and each view's
+    // ratio is warped back from its own phase (:222) and added with weight
+    // lambda/kk, in view order.
+    int image_mc_subset(int k0, int kk, bool hw) {
+        const Geom &g = P.g;
+        const Fields<ST> f = fields();
+        const int v0 = views_img[k0];
+        for (int j = 0; j < kk; j++) {
+            const int v = v0 + j;
+            const float volume = P.volumes[v] - P.volumes[0];
+            const float flow = P.flows[v] - P.flows[0];
+            ST *d = S.img1.as<ST>() + j * V, *dT = S.img1T.as<ST>() + j * V;
+            ctx->label = "warp_fwd";
+            if (hw) {
+                MC_LAUNCH(ctx, (warp_fwd_kernel<SrcTex, ST, ST>), tile_grid(), dim3(32, 8), 0, d,
+                          dT, SrcTex{S.tv_img.tex}, f, g.nx, g.ny, g.nz, volume, flow);
+            } else {
+                MC_LAUNCH(ctx, (warp_fwd_kernel<SrcLinear<float>, ST, ST>), tile_grid(),
+                          dim3(32, 8), 0, d, dT, SrcLinear<float>{P.img}, f, g.nx, g.ny, g.nz,
+                          volume, flow);
+            }
+        }
+        FPVolumes<ST, 1> vol{};
+        vol.std[0] = S.img1.as<ST>();
+        vol.tr[0] = S.img1T.as<ST>();
+        MC_TRY((launch_fp_subset<1, true, ST>(vol, v0, k0, kk, FP_IMAGE, V)));
+        cudaSurfaceObject_t surfs[BP_MAX_VIEWS] = {};
+        for (int j = 0; j < kk; j++) surfs[j] = j == 0 ? S.tv_ratio.surf : S.tv_ratio_sub[j - 1].surf;
+        if (hw)
+            MC_TRY(launch_bp_subset(v0, kk, BP_DIV, nullptr, nullptr, surfs));
+        else
+            MC_TRY(launch_bp_subset(v0, kk, BP_DIV, S.ratio.as<float>(), nullptr, nullptr));
+        const float lam = P.lambda / (float)kk;
+        for (int j = 0; j < kk; j++) {
+            const int v = v0 + j;
+            const float ivolume = P.volumes[0] - P.volumes[v];
+            const float iflow = P.flows[0] - P.flows[v];
+            ctx->label = "warp_back_add";
+            if (hw) {
+                const cudaTextureObject_t t = j == 0 ? S.tv_ratio.tex : S.tv_ratio_sub[j - 1].tex;
+                MC_LAUNCH(ctx, (warp_back_add_kernel<SrcTex, ST>), tile_grid(), dim3(32, 8), 0,
+                          P.img, S.tv_img.surf, SrcTex{t}, f, g.nx, g.ny, g.nz, ivolume, iflow, lam);
+            } else {
+                MC_LAUNCH(ctx, (warp_back_add_kernel<SrcLinear<float>, ST>), tile_grid(),
+                          dim3(32, 8), 0, P.img, (cudaSurfaceObject_t)0,
+                          SrcLinear<float>{S.ratio.as<float>() + j * V}, f, g.nx, g.ny, g.nz,
+                          ivolume, iflow, lam);
+            }
+        }
+        return MCSART_OK;
     }
 
     // AUMISART.cu:184-233 with P = 1.  TEXTURE model: the volume and the
@@ -221,7 +338,13 @@ template <typename ST, int INTERP, int SUM> struct Runner {
         FPVolumes<ST, 1> vol{};
         vol.std[0] = S.img1.as<ST>();
         vol.tr[0] = S.img1T.as<ST>();
-        for (int k = 0; k < (int)views_img.size(); k++) {
+        const int n = (int)views_img.size();
+        for (int k = 0; k < n; k += subset) {
+            const int kk = std::min(subset, n - k);
+            if (kk > 1) {
+                MC_TRY(image_mc_subset(k, kk, hw));
+                continue;
+            }
             const int v = views_img[k];
             const float volume = P.volumes[v] - P.volumes[0];   // :193
             const float flow = P.flows[v] - P.flows[0];
@@ -332,8 +455,8 @@ template <typename ST, int INTERP, int SUM> struct Runner {
             k.insert(k.end(), b, b + n);
         };
         // the storage type itself, not its size: BF16 and F16 are both 2 bytes
-        const int hdr[7] = {kind, opt.storage, INTERP, SUM, groups, (int)P.motion_model,
-                            (int)views_mot.size()};
+        const int hdr[8] = {kind, opt.storage, INTERP, SUM, groups, (int)P.motion_model,
+                            (int)views_mot.size(), subset};
         put(hdr, sizeof(hdr));
         put(views_img.data(), views_img.size() * sizeof(int));
         put(views_mot.data(), views_mot.size() * sizeof(int));
@@ -442,6 +565,10 @@ int validate_options(const mcsart_options &o) {
                "unknown interpolation model %d", o.interp);
     MC_REQUIRE(o.fp_groups >= 0 && o.fp_groups <= 8, "fp_groups must be in [0, 8]");
     MC_REQUIRE(o.fp_sum >= SUM_REF && o.fp_sum <= SUM_KAHAN, "fp_sum must be 0, 1 or 2");
+    MC_REQUIRE(o.subset >= 0 && o.subset <= BP_MAX_VIEWS, "subset must be in [0, %d]",
+               BP_MAX_VIEWS);
+    MC_REQUIRE(o.subset <= 1 || o.fp_sum == SUM_REF,
+               "ordered subsets (subset > 1) use the reference-order projector (fp_sum 0)");
     return MCSART_OK;
 }
 
@@ -465,6 +592,7 @@ MC_EXPORT void mcsart_default_options(mcsart_options *opt) {
     opt->use_graph = 1;
     opt->fp_sum = SUM_REF;
     opt->fp_groups = 0;
+    opt->subset = 1;
 }
 
 MC_EXPORT int mcsart_aumisart_device(mcsart_ctx *ctx, const mcsart_problem *prob, int n_iter,
@@ -562,15 +690,16 @@ MC_EXPORT int mcsart_batch_run(mcsart_ctx *ctx, const mcsart_problem *problems,
     return finish(ctx, "mcsart_batch_run");
 }
 
-MC_EXPORT int mcsart_aumisart(mcsart_ctx *ctx, float *h_outimg, float *h_outproj,
-                              float *h_outnorm, float *h_outalphax, const float *h_img,
-                              const float *h_proj, int nx, int ny, int nz, int na, int nb,
-                              int outIter, int n_views, int n_iter, const int *op_iter, float da,
-                              float db, float ai, float bi, float SO, float SD, float dx,
-                              float lambda, const float *volumes, const float *flows,
-                              const float *err_weights, const float *angles, const float *ax,
-                              const float *ay, const float *az, const float *bx,
-                              const float *by, const float *bz) {
+// host_AUMISART with host pointers; h_out_fields[0..5] receive the final
+// alpha_x, alpha_y, alpha_z, beta_x, beta_y, beta_z (NULL entries skipped).
+static int aumisart_host(mcsart_ctx *ctx, float *h_outimg, float *h_outproj, float *h_outnorm,
+                         float *const *h_out_fields, const float *h_img, const float *h_proj,
+                         int nx, int ny, int nz, int na, int nb, int outIter, int n_views,
+                         int n_iter, const int *op_iter, float da, float db, float ai, float bi,
+                         float SO, float SD, float dx, float lambda, const float *volumes,
+                         const float *flows, const float *err_weights, const float *angles,
+                         const float *ax, const float *ay, const float *az, const float *bx,
+                         const float *by, const float *bz) {
     clear_error();
     (void)outIter; (void)dx; (void)err_weights;  // unused by the reference as well
     MC_TRY(validate_ctx(ctx));
@@ -579,7 +708,7 @@ MC_EXPORT int mcsart_aumisart(mcsart_ctx *ctx, float *h_outimg, float *h_outproj
     g.na = na; g.nb = nb; g.nx = nx; g.ny = ny; g.nz = nz;
     MC_TRY(validate_geom(g));
     MC_TRY(validate_iter(n_views, n_iter, op_iter, angles, volumes, flows));
-    MC_REQUIRE(h_outimg && h_outproj && h_outnorm && h_outalphax && h_img && h_proj,
+    MC_REQUIRE(h_outimg && h_outproj && h_outnorm && h_out_fields[0] && h_img && h_proj,
                "image, projection and output pointers must be non-NULL");
     const bool motion = ax != nullptr;
     MC_REQUIRE(!motion || (ay && az && bx && by && bz),
@@ -626,7 +755,41 @@ MC_EXPORT int mcsart_aumisart(mcsart_ctx *ctx, float *h_outimg, float *h_outproj
     MC_CHECK_CUDA(cudaMemcpyAsync(h_outproj, S.h_resid.ptr, pb, cudaMemcpyDeviceToHost, st));
     MC_CHECK_CUDA(cudaMemcpyAsync(h_outnorm, S.h_norm.ptr, (size_t)n_iter * n_views * sizeof(float),
                                   cudaMemcpyDeviceToHost, st));
-    MC_CHECK_CUDA(cudaMemcpyAsync(h_outalphax, F, vb, cudaMemcpyDeviceToHost, st));
+    for (int c = 0; c < 6; c++)
+        if (h_out_fields[c])
+            MC_CHECK_CUDA(cudaMemcpyAsync(h_out_fields[c], F + c * V, vb, cudaMemcpyDeviceToHost, st));
     MC_CHECK_CUDA(cudaStreamSynchronize(st));
     return MCSART_OK;
+}
+
+MC_EXPORT int mcsart_aumisart(mcsart_ctx *ctx, float *h_outimg, float *h_outproj,
+                              float *h_outnorm, float *h_outalphax, const float *h_img,
+                              const float *h_proj, int nx, int ny, int nz, int na, int nb,
+                              int outIter, int n_views, int n_iter, const int *op_iter, float da,
+                              float db, float ai, float bi, float SO, float SD, float dx,
+                              float lambda, const float *volumes, const float *flows,
+                              const float *err_weights, const float *angles, const float *ax,
+                              const float *ay, const float *az, const float *bx,
+                              const float *by, const float *bz) {
+    float *const out[6] = {h_outalphax, nullptr, nullptr, nullptr, nullptr, nullptr};
+    return aumisart_host(ctx, h_outimg, h_outproj, h_outnorm, out, h_img, h_proj, nx, ny, nz, na,
+                         nb, outIter, n_views, n_iter, op_iter, da, db, ai, bi, SO, SD, dx, lambda,
+                         volumes, flows, err_weights, angles, ax, ay, az, bx, by, bz);
+}
+
+MC_EXPORT int mcsart_aumisart_fields(mcsart_ctx *ctx, float *h_outimg, float *h_outproj,
+                                     float *h_outnorm, float *h_out_ax, float *h_out_ay,
+                                     float *h_out_az, float *h_out_bx, float *h_out_by,
+                                     float *h_out_bz, const float *h_img, const float *h_proj,
+                                     int nx, int ny, int nz, int na, int nb, int outIter,
+                                     int n_views, int n_iter, const int *op_iter, float da,
+                                     float db, float ai, float bi, float SO, float SD, float dx,
+                                     float lambda, const float *volumes, const float *flows,
+                                     const float *err_weights, const float *angles,
+                                     const float *ax, const float *ay, const float *az,
+                                     const float *bx, const float *by, const float *bz) {
+    float *const out[6] = {h_out_ax, h_out_ay, h_out_az, h_out_bx, h_out_by, h_out_bz};
+    return aumisart_host(ctx, h_outimg, h_outproj, h_outnorm, out, h_img, h_proj, nx, ny, nz, na,
+                         nb, outIter, n_views, n_iter, op_iter, da, db, ai, bi, SO, SD, dx, lambda,
+                         volumes, flows, err_weights, angles, ax, ay, az, bx, by, bz);
 }

@@ -38,6 +38,10 @@ struct DriverState {
     // 3D arrays sampled by the texture unit (INTERP_TEXTURE): the volume and
     // the normalised correction of the image pass, and mcsart_deform's source
     TexVol tv_img, tv_ratio, tv_deform;
+    // ordered subsets (options.subset > 1): the corrections of views 2.. of a
+    // subset, and the views' angles on the device
+    TexVol tv_ratio_sub[15];
+    DevBuf angles_dev;
     std::map<int, PassGraph> graphs;  // keyed by pass kind
     void invalidate_graphs() { graphs.clear(); }
 };

@@ -250,6 +250,30 @@ class Context:
                    h(err_weights, name="err_weights") if err_weights is not None else None,
                    h(angles, name="angles"), *[h(f, name="field") for f in (ax, ay, az, bx, by, bz)])
 
+    def aumisart_host(self, img, proj, geo, *, n_iter, op_iter, lambda_, angles, volumes, flows,
+                      fields=None):
+        """host_AUMISART on host arrays through mcsart_aumisart_fields: returns a
+        dict with the image, the residuals of the last image pass, the norm list
+        and all six final DVF fields (alpha_x ... beta_z).  Passing the returned
+        image and fields back continues the reconstruction exactly."""
+        img = np.ascontiguousarray(img, np.float32)
+        proj = np.ascontiguousarray(proj, np.float32)
+        nz, ny, nx = img.shape
+        nv = proj.shape[0]
+        out = dict(img=np.zeros_like(img), resid=np.zeros_like(proj),
+                   norm=np.zeros(int(n_iter) * nv, np.float32),
+                   fields=[np.zeros_like(img) for _ in range(6)])
+        f = [np.ascontiguousarray(x, np.float32) for x in fields] if fields is not None else None
+        keep = [np.ascontiguousarray(x, np.float32) for x in (volumes, flows, angles)]
+        op = np.ascontiguousarray(op_iter, np.int32)
+        self._call("mcsart_aumisart_fields", _hptr(out["img"]), _hptr(out["resid"]),
+                   _hptr(out["norm"]), *[_hptr(x) for x in out["fields"]], _hptr(img), _hptr(proj),
+                   nx, ny, nz, int(geo["na"]), int(geo["nb"]), 1, nv, int(n_iter), _hptr(op),
+                   geo["da"], geo["db"], geo["ai"], geo["bi"], geo["SO"], geo["SD"], 1.0,
+                   float(lambda_), _hptr(keep[0]), _hptr(keep[1]), None, _hptr(keep[2]),
+                   *([_hptr(x) for x in f] if f is not None else [None] * 6))
+        return out
+
     @staticmethod
     def _problem(geo, n_views, lambda_, angles, volumes, flows, img, proj, fields, resid, norm,
                  options):

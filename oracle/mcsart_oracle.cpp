@@ -443,7 +443,8 @@ int aumisart(T *outimg, T *outproj, T *outnorm, T *outalphax, const T *h_img, co
              const int *op_iter, double da, double db, double ai, double bi, double SO, double SD,
              double /*dx*/, double lambda, const float *volumes, const float *flows,
              const float *angles, const T *fax, const T *fay, const T *faz, const T *fbx,
-             const T *fby, const T *fbz, T *fields_out, int tex_mode, int view_lo, int view_hi) {
+             const T *fby, const T *fbz, T *fields_out, int tex_mode, int view_lo, int view_hi,
+             int subset) {
     const int64_t nv = nvox(nx, ny, nz), np = (int64_t)na * nb;
     const bool with_motion = fax != nullptr;  // overload 2
     if (view_hi < 0 || view_hi > n_views) view_hi = n_views;
@@ -470,10 +471,26 @@ int aumisart(T *outimg, T *outproj, T *outnorm, T *outalphax, const T *h_img, co
     };
     for (int it = 0; it < n_iter; it++) {
         if (op_iter[it] == 1) {  // image update, AUMISART.cu:42-64 / :184-234
-            for (int iv = view_lo; iv < view_hi; iv++) {
-                const T *fp_src = img.data();
+            // Ordered subsets of `subset` views (the engine's options.subset):
+            // every view of a subset starts from the image as it was before the
+            // subset, and the image then receives lambda/k times the views'
+            // corrections (static: summed ratios, motion: each back-warped
+            // ratio added in view order).  subset 1 is the reference's loop.
+            const int sub = subset < 1 ? 1 : subset;
+            for (int s0 = view_lo; s0 < view_hi; s0 += sub) {
+                const int kk = std::min(sub, view_hi - s0);
+                std::vector<T> snap;
+                const T *cur = img.data();
+                if (kk > 1) {
+                    snap = img;
+                    cur = snap.data();
+                }
+                const double lam = kk > 1 ? lambda / kk : lambda;
+                std::vector<T> qsum;
+            for (int iv = s0; iv < s0 + kk; iv++) {
+                const T *fp_src = cur;
                 if (with_motion) {
-                    DEF(img1.data(), img.data(), volumes[iv] - volumes[0], flows[iv] - flows[0]);
+                    DEF(img1.data(), cur, volumes[iv] - volumes[0], flows[iv] - flows[0]);
                     fp_src = img1.data();
                 }
                 FP(proj_temp.data(), fp_src, iv);
@@ -491,10 +508,16 @@ int aumisart(T *outimg, T *outproj, T *outnorm, T *outalphax, const T *h_img, co
                 if (with_motion) {
                     DEF(img1.data(), img_temp.data(), volumes[0] - volumes[iv],
                         flows[0] - flows[iv]);
-                    add<T>(img.data(), img1.data(), nx, ny, nz, lambda);
-                } else {
+                    add<T>(img.data(), img1.data(), nx, ny, nz, lam);
+                } else if (kk == 1) {
                     add<T>(img.data(), img_temp.data(), nx, ny, nz, lambda);
+                } else if (iv == s0) {
+                    qsum = img_temp;
+                } else {
+                    add<T>(qsum.data(), img_temp.data(), nx, ny, nz, 1.0);
                 }
+            }
+                if (!with_motion && kk > 1) add<T>(img.data(), qsum.data(), nx, ny, nz, lam);
             }
         } else {  // motion update, AUMISART.cu:66-118 / :236-288
             for (int iv = 1; iv < view_hi; iv += motion_step) {
@@ -609,11 +632,11 @@ int aumisart(T *outimg, T *outproj, T *outnorm, T *outalphax, const T *h_img, co
         const int *op_iter, double da, double db, double ai, double bi, double SO, double SD,  \
         double dx, double lambda, const float *volumes, const float *flows,                    \
         const float *angles, const T *ax, const T *ay, const T *az, const T *bx, const T *by,  \
-        const T *bz, T *fields_out, int tex_mode, int view_lo, int view_hi) {                  \
+        const T *bz, T *fields_out, int tex_mode, int view_lo, int view_hi, int subset) {      \
         return aumisart<T>(outimg, outproj, outnorm, outalphax, img, proj, nx, ny, nz, na, nb, \
                            outIter, n_views, n_iter, op_iter, da, db, ai, bi, SO, SD, dx,      \
                            lambda, volumes, flows, angles, ax, ay, az, bx, by, bz, fields_out, \
-                           tex_mode, view_lo, view_hi);                                        \
+                           tex_mode, view_lo, view_hi, subset);                                \
     }
 
 ORC_DEFINE(double, orc_)

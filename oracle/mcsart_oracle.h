@@ -56,7 +56,8 @@ enum { ORC_TEX_EXACT = 0, ORC_TEX_Q8_NEAREST = 1, ORC_TEX_Q8_TRUNC = 2 };
                     double ai, double bi, double SO, double SD, double dx, double lambda,      \
                     const float *volumes, const float *flows, const float *angles,             \
                     const T *ax, const T *ay, const T *az, const T *bx, const T *by,           \
-                    const T *bz, T *fields_out, int tex_mode, int view_lo, int view_hi);
+                    const T *bz, T *fields_out, int tex_mode, int view_lo, int view_hi,       \
+                    int subset);
 
 ORC_DECL(double, orc_)
 ORC_DECL(float, cpu_)

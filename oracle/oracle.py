@@ -65,7 +65,7 @@ def _declare(L: ctypes.CDLL) -> None:
         getattr(L, pre + "update_udvf").argtypes = [_P] * 8 + [_D, _D, _I, _I, _I, _I]
         getattr(L, pre + "diff").argtypes = [_P, _P, _I, _I, _I, _I]
         f = getattr(L, pre + "aumisart")
-        f.argtypes = ([_P] * 6 + [_I] * 8 + [_P] + [_D] * 8 + [_P] * 3 + [_P] * 6 + [_P, _I, _I, _I])
+        f.argtypes = ([_P] * 6 + [_I] * 8 + [_P] + [_D] * 8 + [_P] * 3 + [_P] * 6 + [_P, _I, _I, _I, _I])
         f.restype = _I
     L.orc_num_threads.restype = _I
     L.orc_set_num_threads.argtypes = [_I]
@@ -227,12 +227,14 @@ def diff(img, ind, prec="orc", init=None):
 
 
 def aumisart(img, proj, geo, it, fields=None, tex_mode=TEX_Q8_NEAREST, prec="orc",
-             view_lo=0, view_hi=-1, return_fields=False):
+             view_lo=0, view_hi=-1, return_fields=False, subset=1):
     """The SART/motion loop of host_AUMISART (src/AUMISART.cu:3 and :143).
 
     ``it`` holds ``n_iter``, ``op_iter``, ``n_views``, ``lambda``, ``volumes``,
     ``flows``, ``angles`` (and optionally ``outIter``); ``fields`` = None selects
-    overload 1 (DVF zero-initialised), a 6-tuple overload 2.
+    overload 1 (DVF zero-initialised), a 6-tuple overload 2.  ``subset`` > 1:
+    the engine's ordered-subset mode (views of a subset start from the same
+    image, which then gets lambda/k times their corrections).
     Returns dict(img, norm, alpha_x, resid[, fields]).
     """
     dt = _dt(prec)
@@ -256,7 +258,8 @@ def aumisart(img, proj, geo, it, fields=None, tex_mode=TEX_Q8_NEAREST, prec="orc
         nb, int(it.get("outIter", 1)), n_views, n_iter, _p(op), float(geo["da"]),
         float(geo["db"]), float(geo["ai"]), float(geo["bi"]), float(geo["SO"]),
         float(geo["SD"]), float(geo.get("dx", 1.0)), float(it["lambda"]), _p(vols), _p(flows),
-        _p(angs), *[_p(x) for x in f], _p(fo), int(tex_mode), int(view_lo), int(view_hi))
+        _p(angs), *[_p(x) for x in f], _p(fo), int(tex_mode), int(view_lo), int(view_hi),
+        int(subset))
     if rc != 0:
         raise RuntimeError(f"oracle aumisart failed: {rc}")
     out = {"img": out_img, "norm": out_norm, "alpha_x": out_ax, "resid": out_proj}

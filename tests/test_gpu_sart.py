@@ -193,3 +193,25 @@ def test_mixed_precision_error_vs_fp64_oracle(ctx, torch_cuda, oracle, storage, 
     err = rel_l2(host(d_img), o["img"])
     print(f"storage={storage} rel L2 vs FP64 oracle after {it['n_iter']} image passes: {err:.3e}")
     assert err <= tol
+
+
+def test_all_fields_returned_and_reconstruction_resumes_exactly(ctx, oracle):
+    """mcsart_aumisart_fields returns all six DVF fields (alpha_x equal to
+    mcsart_aumisart's), and 2 + 2 iterations with the state passed back give
+    the bits of one 4-iteration call."""
+    op = (1, 0, 1, 0)
+    g, it, img0, proj, F = make_case(oracle, motion=True, op_iter=op, seed=6)
+    kw = dict(lambda_=1.0, angles=it["angles"], volumes=it["volumes"], flows=it["flows"])
+    one = ctx.aumisart_host(img0, proj, g, n_iter=4, op_iter=np.array(op, np.int32), fields=F,
+                            **kw)
+    ref = run_engine(ctx, g, it, img0, proj, F)
+    np.testing.assert_array_equal(one["img"], ref["img"])
+    np.testing.assert_array_equal(one["fields"][0], ref["alpha_x"])
+    first = ctx.aumisart_host(img0, proj, g, n_iter=2, op_iter=np.array(op[:2], np.int32),
+                              fields=F, **kw)
+    second = ctx.aumisart_host(first["img"], proj, g, n_iter=2,
+                               op_iter=np.array(op[2:], np.int32), fields=first["fields"], **kw)
+    np.testing.assert_array_equal(second["img"], one["img"])
+    for c in range(6):
+        np.testing.assert_array_equal(second["fields"][c], one["fields"][c])
+    np.testing.assert_array_equal(second["resid"], one["resid"])
