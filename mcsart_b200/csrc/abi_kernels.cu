@@ -48,7 +48,11 @@ int launch_fp_plain(mcsart_ctx *ctx, float *d_proj, const float *d_img, const fl
     a.out = d_proj;
     // the reference's summation order: bitwise the reference kernel's output
     const dim3 grid(div_up(g.na, FPC_COLS), div_up(g.nb, FPC_ROWS), n_views);
-    MC_LAUNCH(ctx, (fp_ref_kernel<K, false, float>), grid, dim3(FPC_THREADS), 0, a);
+    // several views (mcsart_projection_views): the multi-view instantiation
+    if (n_views > 1)
+        MC_LAUNCH(ctx, (fp_ref_kernel<K, false, float, float, true>), grid, dim3(FPC_THREADS), 0, a);
+    else
+        MC_LAUNCH(ctx, (fp_ref_kernel<K, false, float>), grid, dim3(FPC_THREADS), 0, a);
     return MCSART_OK;
 }
 

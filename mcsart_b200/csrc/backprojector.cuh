@@ -195,7 +195,10 @@ __device__ __forceinline__ void bp_gather_view(const BPArgs &p, float angle, con
 // blockDim = (32, BP_ROWS); each thread backprojects the BP_NZ voxels
 // (ix, iy, z0 .. z0 + BP_NZ - 1), z0 = blockIdx.z * BP_NZ, for every view of
 // the launch.
-template <int K, int MODE>
+// MULTI = false: one view (the reference's loop); the view loop and the
+// per-view outputs exist only in the ordered-subset instantiation, so that
+// the single-view kernel keeps its registers (and resident blocks).
+template <int K, int MODE, bool MULTI = false>
 __global__ void __launch_bounds__(256, MCSART_BP_MINBLOCKS) bp_kernel(const BPArgs p) {
     __shared__ float tile[BP_NZ][BP_ROWS][33];
     const Geom &g = p.g;
@@ -204,7 +207,7 @@ __global__ void __launch_bounds__(256, MCSART_BP_MINBLOCKS) bp_kernel(const BPAr
     const int ix = x0 + tx, iy = y0 + ty;
     const bool active = ix < g.nx && iy < g.ny;
     const int64_t plane = (int64_t)g.nx * g.ny, V = plane * g.nz, NP = (int64_t)g.na * g.nb;
-    const int nv = (K == 2 && p.n_views > 1) ? p.n_views : 1;
+    const int nv = MULTI ? p.n_views : 1;
 
     float qsum[BP_NZ];
 #pragma unroll
@@ -213,7 +216,7 @@ __global__ void __launch_bounds__(256, MCSART_BP_MINBLOCKS) bp_kernel(const BPAr
         float acc0[BP_NZ], acc1[BP_NZ];
 #pragma unroll
         for (int k = 0; k < BP_NZ; k++) { acc0[k] = 0.0f; acc1[k] = 0.0f; }
-        const float angle = p.angles ? p.angles[v] : p.angle;
+        const float angle = MULTI ? p.angles[v] : p.angle;
         if (active) bp_gather_view<K>(p, angle, p.proj, p.pair + v * NP, ix, iy, z0, acc0, acc1);
 #pragma unroll
         for (int k = 0; k < BP_NZ; k++) {
@@ -228,10 +231,10 @@ __global__ void __launch_bounds__(256, MCSART_BP_MINBLOCKS) bp_kernel(const BPAr
             if (isnan(q) || isinf(q)) q = 0.0f;     // :21-24
             if (MODE == BP_DIV) {
                 if (p.out) p.out[id + v * V] = q;
-                const cudaSurfaceObject_t s = nv > 1 ? p.outSurfs[v] : p.outSurf;
+                const cudaSurfaceObject_t s = MULTI ? p.outSurfs[v] : p.outSurf;
                 if (s) surf3Dwrite(q, s, ix * (int)sizeof(float), iy, iz, cudaBoundaryModeZero);
             } else {
-                qsum[k] = v == 0 ? q : qsum[k] + q;  // subset: ratios summed in view order
+                qsum[k] = (!MULTI || v == 0) ? q : qsum[k] + q;  // subset: summed in view order
             }
         }
     }

@@ -421,7 +421,10 @@ __device__ __forceinline__ void fp_slab(const RayGeom &r, const Geom &g, const S
 
 // blockDim = FPC_THREADS: thread t is column t % FPC_COLS, row t / FPC_COLS;
 // gridDim = (ceil(na/FPC_COLS), ceil(nb/FPC_ROWS), views).
-template <int K, bool ONES, typename VT, typename MT = VT>
+// MULTI = true: several views per launch (ordered subsets, kernel-level
+// multi-view projection), view = blockIdx.z with the per-view offsets of
+// FPArgs; false: one view per launch without them.
+template <int K, bool ONES, typename VT, typename MT = VT, bool MULTI = false>
 __global__ void __launch_bounds__(FPC_THREADS, FPC_MIN_BLOCKS) fp_ref_kernel(const FPArgs<VT, K, MT> p) {
     __shared__ SlabU sm_u[FPC_CHUNK][FPC_COLS];
     __shared__ double2 sm_norm[FPC_THREADS / 32];
@@ -438,7 +441,7 @@ __global__ void __launch_bounds__(FPC_THREADS, FPC_MIN_BLOCKS) fp_ref_kernel(con
     const VT *base[K];
     int su, sd;
     const int sz = g.nx * g.ny;
-    const int64_t voff = (int64_t)blockIdx.z * p.vol_stride;
+    const int64_t voff = MULTI ? (int64_t)blockIdx.z * p.vol_stride : 0;
     if (r.xdrive) {
         if (p.vol.tr[0] != nullptr) {
 #pragma unroll
@@ -544,7 +547,7 @@ __global__ void __launch_bounds__(FPC_THREADS, FPC_MIN_BLOCKS) fp_ref_kernel(con
     }
 
     const int64_t pix = ia + (int64_t)ib * g.na;
-    const int64_t vpix = pix + (int64_t)blockIdx.z * g.na * g.nb;  // this view's cell
+    const int64_t vpix = MULTI ? pix + (int64_t)blockIdx.z * g.na * g.nb : pix;  // this view's cell
     double nb2 = 0.0, nr2 = 0.0;
     if (active) {
         if (p.mode == FP_PLAIN) {
@@ -579,8 +582,8 @@ __global__ void __launch_bounds__(FPC_THREADS, FPC_MIN_BLOCKS) fp_ref_kernel(con
             tb += sm_norm[w].x;
             tr += sm_norm[w].y;
         }
-        p.norm_part[(int64_t)blockIdx.z * gridDim.x * gridDim.y + blockIdx.y * gridDim.x +
-                    blockIdx.x] = make_double2(tb, tr);
+        const int64_t vblk = MULTI ? (int64_t)blockIdx.z * gridDim.x * gridDim.y : 0;
+        p.norm_part[vblk + blockIdx.y * gridDim.x + blockIdx.x] = make_double2(tb, tr);
     }
 }
 

@@ -32,6 +32,7 @@
 
 namespace mcsart {
 
+
 int fp_auto_groups(int64_t ray_blocks, int n_slabs);
 unsigned stream_blocks(int64_t n);
 
@@ -207,8 +208,8 @@ template <typename ST, int INTERP, int SUM> struct Runner {
         a.norm_part = S.norm_part.as<double2>() + (int64_t)k0 * fp_blocks;
         a.vol_stride = vol_stride;
         ctx->label = mode == FP_MOTION ? "fp_motion" : "fp_image";
-        MC_LAUNCH(ctx, (fp_ref_kernel<K, ONES, VT, ST>), dim3(fp_bx, fp_by, kk), dim3(FPC_THREADS),
-                  0, a);
+        MC_LAUNCH(ctx, (fp_ref_kernel<K, ONES, VT, ST, true>), dim3(fp_bx, fp_by, kk),
+                  dim3(FPC_THREADS), 0, a);
         return MCSART_OK;
     }
 
@@ -231,10 +232,10 @@ template <typename ST, int INTERP, int SUM> struct Runner {
             block(32, BP_ROWS);
         if (mode == BP_DIV) {
             ctx->label = "bp_div";
-            MC_LAUNCH(ctx, (bp_kernel<2, BP_DIV>), grid, block, 0, b);
+            MC_LAUNCH(ctx, (bp_kernel<2, BP_DIV, true>), grid, block, 0, b);
         } else {
             ctx->label = "bp_div_add";
-            MC_LAUNCH(ctx, (bp_kernel<2, BP_DIV_ADD>), grid, block, 0, b);
+            MC_LAUNCH(ctx, (bp_kernel<2, BP_DIV_ADD, true>), grid, block, 0, b);
         }
         return MCSART_OK;
     }
