@@ -92,6 +92,15 @@ int mcsart_projection(mcsart_ctx *ctx, float *d_proj, const float *d_img, float 
 int mcsart_backprojection(mcsart_ctx *ctx, float *d_img, const float *d_proj, float angle,
                           float SO, float SD, float da, int na, float ai, float db, int nb,
                           float bi, int nx, int ny, int nz);
+/* The exact adjoint (transpose) of mcsart_projection, same arguments as
+ * mcsart_backprojection (d_img is overwritten).  No counterpart in the
+ * reference: its backprojector (src/cu_backprojection.cu) is a different
+ * operator, not the projector's transpose.  Deterministic gather with the
+ * projector's own weights; <mcsart_projection(x), y> = <x, adjoint(y)> up to
+ * FP32 rounding of the sums. */
+int mcsart_backprojection_adjoint(mcsart_ctx *ctx, float *d_img, const float *d_proj,
+                                  float angle, float SO, float SD, float da, int na, float ai,
+                                  float db, int nb, float bi, int nx, int ny, int nz);
 /* replaces host_deform, include/cu_deform.h:8 (src/cu_deform.cu:3); d_img1 may
  * equal d_img */
 int mcsart_deform(mcsart_ctx *ctx, float *d_img1, const float *d_img, int nx, int ny, int nz,

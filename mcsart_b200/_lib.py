@@ -61,6 +61,7 @@ SIGNATURES = {
     # first argument is a cudaStream_t here, not a context
     "mcsart_projection_noalloc": [_P, _P] + _GEO,
     "mcsart_backprojection": [_P, _P] + _GEO,
+    "mcsart_backprojection_adjoint": [_P, _P] + _GEO,
     "mcsart_deform": [_P, _P, _I, _I, _I, _F, _F] + [_P] * 6,
     "mcsart_deform2": [_P, _P, _I, _I, _I, _F, _F] + [_P] * 6,
     "mcsart_forward_dvf": [_P] * 9 + [_F, _F, _I, _I, _I],

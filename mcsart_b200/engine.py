@@ -152,6 +152,13 @@ class Context:
         self._call("mcsart_backprojection", _ptr(d_img, "d_img", 4), _ptr(d_proj, "d_proj", 4),
                    angle, SO, SD, da, na, ai, db, nb, bi, nx, ny, nz)
 
+    def host_backprojection_adjoint(self, d_img, d_proj, angle, SO, SD, da, na, ai, db, nb, bi,
+                                    nx, ny, nz):
+        """Exact adjoint of host_projection (mcsart_backprojection_adjoint); no
+        counterpart in the reference."""
+        self._call("mcsart_backprojection_adjoint", _ptr(d_img, "d_img", 4),
+                   _ptr(d_proj, "d_proj", 4), angle, SO, SD, da, na, ai, db, nb, bi, nx, ny, nz)
+
     def host_deform(self, d_img1, d_img, nx, ny, nz, volume, flow, alpha_x, alpha_y, alpha_z,
                     beta_x, beta_y, beta_z):
         """include/cu_deform.h:8"""

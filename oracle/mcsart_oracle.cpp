@@ -40,9 +40,12 @@ inline int64_t nvox(int nx, int ny, int nz) { return (int64_t)nx * ny * nz; }
 
 // ---------------------------------------------------------------- projector
 // src/cu_projection.cu:15-145: one detector cell (ia, ib) of one view.
-template <typename T>
-T project_ray(const T *img, int ia, int ib, float anglef, T SO, T SD, T da, T ai, T db, T bi,
-              int nx, int ny, int nz) {
+// The terms of one ray (src/cu_projection.cu:22-144): visit(voxel index,
+// in-plane weight, axial weight) in the reference's order.  project_ray sums
+// img * w_u * w_z over them; the exact adjoint scatters p * w_u * w_z.
+template <typename T, typename Visit>
+void ray_walk(int ia, int ib, float anglef, T SO, T SD, T da, T ai, T db, T bi, int nx, int ny,
+              int nz, Visit visit) {
     // Driving-axis decision in float, as the reference evaluates it (:23-39).
     const float cf = std::cos(anglef), sf = std::sin(anglef);
     const float SOf = (float)SO, SDf = (float)SD, daf = (float)da, aif = (float)ai;
@@ -60,7 +63,6 @@ T project_ray(const T *img, int ia, int ib, float anglef, T SO, T SD, T da, T ai
     const T z2 = ((T)ib + bi) * db;                               // :32
     const T x21 = x2 - x1, y21 = y2 - y1, z21 = z2 - z1;          // :34-36
     const T half_da = da / 2, half_db = db / 2;
-    T acc = 0;
     if (xdrive) {
         for (int ix = 0; ix < nx; ix++) {                          // :44
             const T xl = x21 - half_da * sphi, xr = x21 + half_da * sphi;  // :48-49
@@ -80,7 +82,7 @@ T project_ray(const T *img, int ia, int ib, float anglef, T SO, T SD, T da, T ai
                 const T wy = (tmin((T)iy + 1, yi2) - tmax((T)iy, yi1)) / (yi2 - yi1);
                 for (int iz = std::max(0, Zi1); iz <= std::min(nz - 1, Zi2); iz++) { // :84
                     const T wz = (tmin((T)iz + 1, zi2) - tmax((T)iz, zi1)) / (zi2 - zi1);
-                    acc += img[ix + (int64_t)iy * nx + (int64_t)iz * nx * ny] * wy * wz;  // :87
+                    visit(ix + (int64_t)iy * nx + (int64_t)iz * nx * ny, wy, wz);  // :87
                 }
             }
         }
@@ -103,12 +105,38 @@ T project_ray(const T *img, int ia, int ib, float anglef, T SO, T SD, T da, T ai
                 const T wx = (tmin((T)ix + 1, xi2) - tmax((T)ix, xi1)) / (xi2 - xi1);
                 for (int iz = std::max(0, Zi1); iz <= std::min(nz - 1, Zi2); iz++) { // :137
                     const T wz = (tmin((T)iz + 1, zi2) - tmax((T)iz, zi1)) / (zi2 - zi1);
-                    acc += img[ix + (int64_t)iy * nx + (int64_t)iz * nx * ny] * wx * wz;  // :140
+                    visit(ix + (int64_t)iy * nx + (int64_t)iz * nx * ny, wx, wz);  // :140
                 }
             }
         }
     }
+}
+
+template <typename T>
+T project_ray(const T *img, int ia, int ib, float anglef, T SO, T SD, T da, T ai, T db, T bi,
+              int nx, int ny, int nz) {
+    T acc = 0;
+    ray_walk<T>(ia, ib, anglef, SO, SD, da, ai, db, bi, nx, ny, nz,
+                [&](int64_t i, T wu, T wz) { acc += img[i] * wu * wz; });
     return acc;
+}
+
+// Exact adjoint (transpose) of projection(): img = A^T proj, scattered ray by
+// ray in the reference projector's terms.  Not a reference function (its
+// backprojector is a different operator); the engine's
+// mcsart_backprojection_adjoint is checked against it.
+template <typename T>
+void backprojection_adjoint(T *img, const T *proj, double angle, double SO, double SD, double da,
+                            int na, double ai, double db, int nb, double bi, int nx, int ny,
+                            int nz) {
+    const float anglef = (float)angle;
+    std::fill(img, img + nvox(nx, ny, nz), (T)0);
+    for (int ib = 0; ib < nb; ib++)
+        for (int ia = 0; ia < na; ia++) {
+            const T p = proj[ia + (int64_t)ib * na];
+            ray_walk<T>(ia, ib, anglef, (T)SO, (T)SD, (T)da, (T)ai, (T)db, (T)bi, nx, ny, nz,
+                        [&](int64_t i, T wu, T wz) { img[i] += p * wu * wz; });
+        }
 }
 
 template <typename T>
@@ -569,6 +597,13 @@ int aumisart(T *outimg, T *outproj, T *outnorm, T *outalphax, const T *h_img, co
                                   double da, int na, double ai, double db, int nb, double bi,  \
                                   int nx, int ny, int nz) {                                    \
         projection<T>(proj, img, angle, SO, SD, da, na, ai, db, nb, bi, nx, ny, nz);           \
+    }                                                                                          \
+    extern "C" void P##backprojection_adjoint(T *img, const T *proj, double angle, double SO,  \
+                                              double SD, double da, int na, double ai,         \
+                                              double db, int nb, double bi, int nx, int ny,    \
+                                              int nz) {                                        \
+        backprojection_adjoint<T>(img, proj, angle, SO, SD, da, na, ai, db, nb, bi, nx, ny,     \
+                                  nz);                                                         \
     }                                                                                          \
     extern "C" void P##backprojection(T *img, const T *proj, double angle, double SO,          \
                                       double SD, double da, int na, double ai, double db,      \

@@ -23,6 +23,9 @@ enum { ORC_TEX_EXACT = 0, ORC_TEX_Q8_NEAREST = 1, ORC_TEX_Q8_TRUNC = 2 };
     void P##projection(T *proj, const T *img, double angle, double SO, double SD, double da,   \
                        int na, double ai, double db, int nb, double bi, int nx, int ny,        \
                        int nz);                                                                \
+    void P##backprojection_adjoint(T *img, const T *proj, double angle, double SO, double SD,  \
+                                   double da, int na, double ai, double db, int nb, double bi, \
+                                   int nx, int ny, int nz);                                    \
     void P##backprojection(T *img, const T *proj, double angle, double SO, double SD,          \
                            double da, int na, double ai, double db, int nb, double bi, int nx, \
                            int ny, int nz);                                                    \

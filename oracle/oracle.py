@@ -52,6 +52,7 @@ def _declare(L: ctypes.CDLL) -> None:
         geo = [_D, _D, _D, _D, _I, _D, _D, _I, _D, _I, _I, _I]
         getattr(L, pre + "projection").argtypes = [_P, _P] + geo
         getattr(L, pre + "backprojection").argtypes = [_P, _P] + geo
+        getattr(L, pre + "backprojection_adjoint").argtypes = [_P, _P] + geo
         getattr(L, pre + "backprojection_sc").argtypes = [_P, _P, _D] + geo
         getattr(L, pre + "forward_dvf").argtypes = [_P] * 9 + [_D, _D, _I, _I, _I]
         getattr(L, pre + "deform").argtypes = [_P, _P, _I, _I, _I, _D, _D] + [_P] * 6 + [_I]
@@ -111,6 +112,14 @@ def backprojection(proj, angle, geo, prec="orc"):
     proj = _arr(proj, prec)
     out = np.zeros((geo["nz"], geo["ny"], geo["nx"]), _dt(prec))
     getattr(lib(), prec + "_backprojection")(_p(out), _p(proj), float(angle), *_geo(geo))
+    return out
+
+
+def backprojection_adjoint(proj, angle, geo, prec="orc"):
+    """Exact adjoint (transpose) of projection(): scatters each ray's terms."""
+    proj = _arr(proj, prec)
+    out = np.zeros((geo["nz"], geo["ny"], geo["nx"]), _dt(prec))
+    getattr(lib(), prec + "_backprojection_adjoint")(_p(out), _p(proj), float(angle), *_geo(geo))
     return out
 
 

@@ -106,3 +106,18 @@ def test_static_loop_fp32_port_tracks_fp64(oracle):
     o32 = oracle.aumisart(np.zeros_like(truth), proj, g, it, None, prec="cpu")
     assert rel_l2(o32["img"], o64["img"]) <= 1e-5
     assert o64["norm"][-10:].mean() < o64["norm"][:10].mean()
+
+
+def test_oracle_adjoint_is_the_transpose_of_the_oracle_projection(oracle):
+    """<A x, y> = <x, A^T y> for the FP64 oracle's projector and its adjoint."""
+    import numpy as np
+    from conftest import geo
+    g = geo(nx=20, ny=18, nz=12, na=30, nb=20)
+    rng = np.random.default_rng(5)
+    x = rng.random((g["nz"], g["ny"], g["nx"]))
+    y = rng.random((g["nb"], g["na"]))
+    for a in (0.0, 0.5, 0.7853982, 2.2, 3.9, 5.6):
+        ax = oracle.projection(x, a, g)
+        aty = oracle.backprojection_adjoint(y, a, g)
+        lhs, rhs = float(np.sum(ax * y)), float(np.sum(x * aty))
+        assert abs(lhs - rhs) <= 1e-12 * abs(lhs), (a, lhs, rhs)
