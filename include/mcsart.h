@@ -117,6 +117,17 @@ int mcsart_forward_dvf(mcsart_ctx *ctx, float *mx, float *my, float *mz, const f
                        const float *alpha_y, const float *alpha_z, const float *beta_x,
                        const float *beta_y, const float *beta_z, float volume, float flow,
                        int nx, int ny, int nz);
+/* The inverse of the warp's displacement m = alpha*volume + beta*flow (as
+ * computed by mcsart_forward_dvf), for square slices: a fixed-point iteration
+ * n(q) = -D(q + n(q)) from n = 0, n_iter steps, exact FP32 trilinear samples,
+ * written in the layout of mcsart_forward_dvf (inv_x, inv_y, inv_z), so that
+ * warping with it undoes the warp with m.  The reference approximates the
+ * inverse by negating volume and flow (src/AUMISART.cu:222); a fixed-point
+ * inverse appears only in its unused waste/kernel_invertDVF.cu. */
+int mcsart_invert_dvf(mcsart_ctx *ctx, float *inv_x, float *inv_y, float *inv_z,
+                      const float *alpha_x, const float *alpha_y, const float *alpha_z,
+                      const float *beta_x, const float *beta_y, const float *beta_z, float volume,
+                      float flow, int nx, int ny, int nz, int n_iter);
 /* replaces host_add, include/cu_add.h:4 (src/cu_add.cu:2) */
 int mcsart_add(mcsart_ctx *ctx, float *img1, const float *img, int nx, int ny, int nz,
                float weight);
@@ -186,6 +197,10 @@ typedef struct {
                          image, in one projector and one backprojector launch, and the
                          image receives lambda/k times their sum (a different
                          algorithm from the reference's, not a drop-in) */
+    int dvf_inverse;  /* image passes with motion: 0 = warp corrections back with the
+                         negated amplitudes (the reference); n > 0 = with the true
+                         inverse of each view's displacement, n fixed-point steps
+                         (mcsart_invert_dvf; FP32 storage, square slices; not a drop-in) */
 } mcsart_options;
 void mcsart_default_options(mcsart_options *opt);
 

@@ -35,7 +35,8 @@ class McsartError(RuntimeError):
 
 class Options(ctypes.Structure):
     _fields_ = [("storage", ctypes.c_int), ("interp", ctypes.c_int), ("use_graph", ctypes.c_int),
-                ("fp_sum", ctypes.c_int), ("fp_groups", ctypes.c_int), ("subset", ctypes.c_int)]
+                ("fp_sum", ctypes.c_int), ("fp_groups", ctypes.c_int), ("subset", ctypes.c_int),
+                ("dvf_inverse", ctypes.c_int)]
 
 
 class Problem(ctypes.Structure):
@@ -64,6 +65,7 @@ SIGNATURES = {
     "mcsart_backprojection_adjoint": [_P, _P] + _GEO,
     "mcsart_deform": [_P, _P, _I, _I, _I, _F, _F] + [_P] * 6,
     "mcsart_deform2": [_P, _P, _I, _I, _I, _F, _F] + [_P] * 6,
+    "mcsart_invert_dvf": [_P] * 9 + [_F, _F, _I, _I, _I, _I],
     "mcsart_forward_dvf": [_P] * 9 + [_F, _F, _I, _I, _I],
     "mcsart_add": [_P, _P, _I, _I, _I, _F],
     "mcsart_add2": [_P, _P, _I, _I, _I, _P, _F, _I],

@@ -210,6 +210,29 @@ MC_EXPORT int mcsart_forward_dvf(mcsart_ctx *ctx, float *mx, float *my, float *m
     return finish(ctx, "mcsart_forward_dvf");
 }
 
+MC_EXPORT int mcsart_invert_dvf(mcsart_ctx *ctx, float *inv_x, float *inv_y, float *inv_z,
+                                const float *ax, const float *ay, const float *az,
+                                const float *bx, const float *by, const float *bz, float volume,
+                                float flow, int nx, int ny, int nz, int n_iter) {
+    clear_error();
+    MC_TRY(validate_ctx(ctx));
+    MC_TRY(validate_dims(nx, ny, nz));
+    MC_REQUIRE(inv_x && inv_y && inv_z && ax && ay && az && bx && by && bz,
+               "pointers must be non-NULL");
+    MC_REQUIRE(nx == ny, "the warp is a displacement field only for square slices (nx == ny)");
+    MC_REQUIRE(n_iter >= 1 && n_iter <= 64, "n_iter must be in [1, 64]");
+    const int64_t n = nvox(nx, ny, nz);
+    void *ws;
+    MC_TRY(workspace(ctx, "inv_m", 3 * n * sizeof(float), &ws));
+    float *m = (float *)ws;
+    const Fields<float> f{ax, ay, az, bx, by, bz};
+    MC_LAUNCH(ctx, forward_dvf_kernel, stream_blocks(n), 256, 0, m, m + n, m + 2 * n, f, n, volume,
+              flow);
+    MC_LAUNCH(ctx, invert_dvf_kernel, dim3(div_up(nx, 32), div_up(ny, 8), nz), dim3(32, 8), 0,
+              inv_x, inv_y, inv_z, m, m + n, m + 2 * n, nx, ny, nz, n_iter);
+    return finish(ctx, "mcsart_invert_dvf");
+}
+
 MC_EXPORT int mcsart_add(mcsart_ctx *ctx, float *img1, const float *img, int nx, int ny, int nz,
                          float weight) {
     clear_error();

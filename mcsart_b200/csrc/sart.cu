@@ -84,6 +84,7 @@ template <typename ST, int INTERP, int SUM> struct Runner {
     int64_t V = 0, NP = 0;
     int fp_bx = 0, fp_by = 0, fp_blocks = 0, groups = 1;
     int subset = 1;  // views per ordered subset in image passes
+    int inv_iters = 0;  // fixed-point steps of the true DVF inverse (0: negated amplitudes)
     std::vector<int> views_img, views_mot;
 
     Runner(mcsart_ctx *c, const Problem &p, const mcsart_options &o)
@@ -97,6 +98,7 @@ template <typename ST, int INTERP, int SUM> struct Runner {
                  : opt.fp_groups > 0 ? std::min(opt.fp_groups, 8)
                                      : fp_auto_groups(fp_blocks, std::max(P.g.nx, P.g.ny));
         subset = std::min(std::max(opt.subset, 1), BP_MAX_VIEWS);
+        inv_iters = P.motion_model ? opt.dvf_inverse : 0;
         for (int v = 0; v < P.n_views; v++) views_img.push_back(v);
         const int step = P.motion_model ? 1 : 10;  // AUMISART.cu:242 vs :72
         for (int v = 1; v < P.n_views; v += step) views_mot.push_back(v);
@@ -126,6 +128,10 @@ template <typename ST, int INTERP, int SUM> struct Runner {
             MC_TRY(S.tv_ratio.ensure(P.g.nx, P.g.ny, P.g.nz));
             for (int j = 1; j < subset; j++)
                 MC_TRY(S.tv_ratio_sub[j - 1].ensure(P.g.nx, P.g.ny, P.g.nz));
+        }
+        if (inv_iters > 0) {
+            MC_TRY(S.m3.ensure(3 * vf));
+            MC_TRY(S.inv3.ensure(3 * vf));
         }
         MC_TRY(S.angles_dev.ensure((size_t)P.n_views * sizeof(float)));
         MC_CHECK_CUDA(cudaMemcpyAsync(S.angles_dev.ptr, P.angles, P.n_views * sizeof(float),
@@ -272,6 +278,52 @@ template <typename ST, int INTERP, int SUM> struct Runner {
         return finalize_norms(S.views_image.as<int>(), (int)views_img.size());
     }
 
+    // The image pass's correction of view v, sampled from `tex` (texture
+    // model) or `lin`, warped back to the reference phase and added with
+    // weight lam: with the negated amplitudes (:222) or, with options
+    // dvf_inverse, with the true inverse of the view's displacement.
+    int back_warp_add(int v, bool hw, cudaTextureObject_t tex, const float *lin, float lam) {
+        const Geom &g = P.g;
+        const Fields<ST> f = fields();
+        if (inv_iters > 0) {  // FP32 fields (validated)
+            const float *F = (const float *)P.fields;
+            const Fields<float> ff{F, F + V, F + 2 * V, F + 3 * V, F + 4 * V, F + 5 * V};
+            const float volume = P.volumes[v] - P.volumes[0];
+            const float flow = P.flows[v] - P.flows[0];
+            float *m = S.m3.as<float>(), *n = S.inv3.as<float>();
+            ctx->label = "dvf_inverse";
+            MC_LAUNCH(ctx, forward_dvf_kernel, stream_blocks(V), 256, 0, m, m + V, m + 2 * V, ff,
+                      V, volume, flow);
+            ctx->label = "dvf_inverse";
+            MC_LAUNCH(ctx, invert_dvf_kernel, dim3(div_up(g.nx, 32), div_up(g.ny, 8), g.nz),
+                      dim3(32, 8), 0, n, n + V, n + 2 * V, m, m + V, m + 2 * V, g.nx, g.ny, g.nz,
+                      inv_iters);
+            ctx->label = "warp_back_add";
+            if (hw) {
+                MC_LAUNCH(ctx, warp_back_add_disp_kernel<SrcTex>, tile_grid(), dim3(32, 8), 0,
+                          P.img, S.tv_img.surf, SrcTex{tex}, n, n + V, n + 2 * V, g.nx, g.ny,
+                          g.nz, lam);
+            } else {
+                MC_LAUNCH(ctx, warp_back_add_disp_kernel<SrcLinear<float>>, tile_grid(),
+                          dim3(32, 8), 0, P.img, (cudaSurfaceObject_t)0, SrcLinear<float>{lin}, n,
+                          n + V, n + 2 * V, g.nx, g.ny, g.nz, lam);
+            }
+            return MCSART_OK;
+        }
+        const float ivolume = P.volumes[0] - P.volumes[v];  // :222
+        const float iflow = P.flows[0] - P.flows[v];
+        ctx->label = "warp_back_add";
+        if (hw) {
+            MC_LAUNCH(ctx, (warp_back_add_kernel<SrcTex, ST>), tile_grid(), dim3(32, 8), 0, P.img,
+                      S.tv_img.surf, SrcTex{tex}, f, g.nx, g.ny, g.nz, ivolume, iflow, lam);
+        } else {
+            MC_LAUNCH(ctx, (warp_back_add_kernel<SrcLinear<float>, ST>), tile_grid(), dim3(32, 8),
+                      0, P.img, (cudaSurfaceObject_t)0, SrcLinear<float>{lin}, f, g.nx, g.ny,
+                      g.nz, ivolume, iflow, lam);
+        }
+        return MCSART_OK;
+    }
+
     // Ordered subset of kk > 1 views in the motion-compensated image pass:
     // every view warps the same image to its phase (:193), one projector
     // launch and one backprojector launch serve the kk views, and each view's
@@ -308,20 +360,8 @@ template <typename ST, int INTERP, int SUM> struct Runner {
             MC_TRY(launch_bp_subset(v0, kk, BP_DIV, S.ratio.as<float>(), nullptr, nullptr));
         const float lam = P.lambda / (float)kk;
         for (int j = 0; j < kk; j++) {
-            const int v = v0 + j;
-            const float ivolume = P.volumes[0] - P.volumes[v];
-            const float iflow = P.flows[0] - P.flows[v];
-            ctx->label = "warp_back_add";
-            if (hw) {
-                const cudaTextureObject_t t = j == 0 ? S.tv_ratio.tex : S.tv_ratio_sub[j - 1].tex;
-                MC_LAUNCH(ctx, (warp_back_add_kernel<SrcTex, ST>), tile_grid(), dim3(32, 8), 0,
-                          P.img, S.tv_img.surf, SrcTex{t}, f, g.nx, g.ny, g.nz, ivolume, iflow, lam);
-            } else {
-                MC_LAUNCH(ctx, (warp_back_add_kernel<SrcLinear<float>, ST>), tile_grid(),
-                          dim3(32, 8), 0, P.img, (cudaSurfaceObject_t)0,
-                          SrcLinear<float>{S.ratio.as<float>() + j * V}, f, g.nx, g.ny, g.nz,
-                          ivolume, iflow, lam);
-            }
+            const cudaTextureObject_t t = j == 0 ? S.tv_ratio.tex : S.tv_ratio_sub[j - 1].tex;
+            MC_TRY(back_warp_add(v0 + j, hw, t, S.ratio.as<float>() + j * V, lam));
         }
         return MCSART_OK;
     }
@@ -364,19 +404,7 @@ template <typename ST, int INTERP, int SUM> struct Runner {
                 MC_TRY(launch_bp(v, BP_DIV, nullptr, nullptr, S.tv_ratio.surf));
             else
                 MC_TRY(launch_bp(v, BP_DIV, S.ratio.as<float>(), nullptr));
-            const float ivolume = P.volumes[0] - P.volumes[v];  // :222
-            const float iflow = P.flows[0] - P.flows[v];
-            ctx->label = "warp_back_add";
-            if (hw) {
-                MC_LAUNCH(ctx, (warp_back_add_kernel<SrcTex, ST>), tile_grid(), dim3(32, 8), 0,
-                          P.img, S.tv_img.surf, SrcTex{S.tv_ratio.tex}, f, g.nx, g.ny, g.nz,
-                          ivolume, iflow, P.lambda);
-            } else {
-                MC_LAUNCH(ctx, (warp_back_add_kernel<SrcLinear<float>, ST>), tile_grid(), dim3(32, 8),
-                          0, P.img, (cudaSurfaceObject_t)0,
-                          SrcLinear<float>{S.ratio.as<float>()}, f, g.nx, g.ny, g.nz, ivolume,
-                          iflow, P.lambda);
-            }
+            MC_TRY(back_warp_add(v, hw, S.tv_ratio.tex, S.ratio.as<float>(), P.lambda));
         }
         return finalize_norms(S.views_image.as<int>(), (int)views_img.size());
     }
@@ -456,8 +484,8 @@ template <typename ST, int INTERP, int SUM> struct Runner {
             k.insert(k.end(), b, b + n);
         };
         // the storage type itself, not its size: BF16 and F16 are both 2 bytes
-        const int hdr[8] = {kind, opt.storage, INTERP, SUM, groups, (int)P.motion_model,
-                            (int)views_mot.size(), subset};
+        const int hdr[9] = {kind, opt.storage, INTERP, SUM, groups, (int)P.motion_model,
+                            (int)views_mot.size(), subset, inv_iters};
         put(hdr, sizeof(hdr));
         put(views_img.data(), views_img.size() * sizeof(int));
         put(views_mot.data(), views_mot.size() * sizeof(int));
@@ -570,6 +598,9 @@ int validate_options(const mcsart_options &o) {
                BP_MAX_VIEWS);
     MC_REQUIRE(o.subset <= 1 || o.fp_sum == SUM_REF,
                "ordered subsets (subset > 1) use the reference-order projector (fp_sum 0)");
+    MC_REQUIRE(o.dvf_inverse >= 0 && o.dvf_inverse <= 64, "dvf_inverse must be in [0, 64]");
+    MC_REQUIRE(o.dvf_inverse == 0 || o.storage == MCSART_F32,
+               "the true DVF inverse (dvf_inverse > 0) needs FP32 storage");
     return MCSART_OK;
 }
 
@@ -594,6 +625,7 @@ MC_EXPORT void mcsart_default_options(mcsart_options *opt) {
     opt->fp_sum = SUM_REF;
     opt->fp_groups = 0;
     opt->subset = 1;
+    opt->dvf_inverse = 0;
 }
 
 MC_EXPORT int mcsart_aumisart_device(mcsart_ctx *ctx, const mcsart_problem *prob, int n_iter,
@@ -612,6 +644,8 @@ MC_EXPORT int mcsart_aumisart_device(mcsart_ctx *ctx, const mcsart_problem *prob
     MC_TRY(validate_iter(prob->n_views, n_iter, h_op_iter, prob->h_angles, prob->h_volumes,
                          prob->h_flows));
     MC_REQUIRE(prob->d_img && prob->d_proj, "d_img and d_proj must be non-NULL");
+    MC_REQUIRE(opt.dvf_inverse == 0 || prob->d_fields == nullptr || prob->nx == prob->ny,
+               "the true DVF inverse (dvf_inverse > 0) needs square slices (nx == ny)");
     if (!ctx->driver) ctx->driver.reset(new DriverState());
     DriverState &S = *ctx->driver;
     const int64_t V = nvox(g.nx, g.ny, g.nz);

@@ -42,6 +42,8 @@ struct DriverState {
     // subset, and the views' angles on the device
     TexVol tv_ratio_sub[15];
     DevBuf angles_dev;
+    // options.dvf_inverse > 0: a view's forward displacement and its inverse
+    DevBuf m3, inv3;
     std::map<int, PassGraph> graphs;  // keyed by pass kind
     void invalidate_graphs() { graphs.clear(); }
 };

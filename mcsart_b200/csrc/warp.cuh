@@ -173,4 +173,62 @@ static __global__ void __launch_bounds__(256) warp_back_add_kernel(
     }
 }
 
+// Inverse of the warp's displacement, for square slices (nx == ny), where
+// the reference's warp (cu_deform.cu:79-90) samples memory position
+// q = (X, Y, Z) of its source at q + D(q) with D = (my, mx, mz)(q) (the
+// in-slice transposed index swaps the first two components).  The inverse
+// N(q) = -D(q + N(q)) is found by fixed-point iteration from N = 0 with exact
+// FP32 trilinear samples of m (clamped at the edges, as the texture), and
+// returned in the forward layout: ox = N_Y, oy = N_X, oz = N_Z, so that a
+// warp with displacement (ox, oy, oz) undoes the warp with (mx, my, mz).
+// blockDim (32, 8), 32x8 tiles of slice blockIdx.z.
+static __global__ void __launch_bounds__(256) invert_dvf_kernel(
+    float *ox, float *oy, float *oz, const float *mx, const float *my, const float *mz, int nx,
+    int ny, int nz, int iters) {
+    const int X = blockIdx.x * 32 + threadIdx.x, Y = blockIdx.y * 8 + threadIdx.y, Z = blockIdx.z;
+    if (X >= nx || Y >= ny) return;
+    const SrcLinear<float> sx{my}, sy{mx}, sz{mz};
+    float NX = 0.0f, NY = 0.0f, NZ = 0.0f;
+    for (int k = 0; k < iters; k++) {
+        const float px = (float)X + 0.5f + NX, py = (float)Y + 0.5f + NY, pz = (float)Z + 0.5f + NZ;
+        const float dX = sx.fetch(px, py, pz, nx, ny, nz);
+        const float dY = sy.fetch(px, py, pz, nx, ny, nz);
+        const float dZ = sz.fetch(px, py, pz, nx, ny, nz);
+        NX = -dX;
+        NY = -dY;
+        NZ = -dZ;
+    }
+    const int64_t id = X + (int64_t)Y * nx + (int64_t)Z * nx * ny;
+    ox[id] = NY;
+    oy[id] = NX;
+    oz[id] = NZ;
+}
+
+// warp_back_add_kernel with an explicit displacement (mx, my, mz) instead of
+// alpha * volume + beta * flow: img += lambda * src sampled at the warped
+// position (square slices).  blockDim (32, 8), 32x32 tiles of slice blockIdx.z.
+template <typename SRC>
+static __global__ void __launch_bounds__(256) warp_back_add_disp_kernel(
+    float *img, cudaSurfaceObject_t img_surf, const SRC src, const float *mx, const float *my,
+    const float *mz, int nx, int ny, int nz, float lambda) {
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int xm = blockIdx.x * 32 + tx, iz = blockIdx.z;
+    const int64_t slice = (int64_t)iz * nx * ny;
+    if (xm >= nx) return;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const int ym = blockIdx.y * 32 + ty + 8 * k;
+        if (ym >= ny) break;
+        const int64_t id = xm + (int64_t)ym * nx + slice;
+        int ix, iy;
+        warp_coords(xm, ym, nx, ny, ix, iy);
+        const float xi = iy + 1.0f + my[id], yi = ix + 1.0f + mx[id], zi = iz + 1.0f + mz[id];
+        const float w = src.fetch(xi - 0.5f, yi - 0.5f, zi - 0.5f, nx, ny, nz);
+        const float v = __fmaf_rn(w, lambda, img[id]);  // cu_add.cu:17
+        img[id] = v;
+        if (img_surf)
+            surf3Dwrite(v, img_surf, xm * (int)sizeof(float), ym, iz, cudaBoundaryModeZero);
+    }
+}
+
 }  // namespace mcsart

@@ -152,6 +152,14 @@ class Context:
         self._call("mcsart_backprojection", _ptr(d_img, "d_img", 4), _ptr(d_proj, "d_proj", 4),
                    angle, SO, SD, da, na, ai, db, nb, bi, nx, ny, nz)
 
+    def invert_dvf(self, inv_x, inv_y, inv_z, alpha_x, alpha_y, alpha_z, beta_x, beta_y, beta_z,
+                   volume, flow, nx, ny, nz, n_iter):
+        """True inverse of the warp's displacement (mcsart_invert_dvf); no counterpart in
+        the reference, which negates the amplitudes (src/AUMISART.cu:222)."""
+        self._call("mcsart_invert_dvf", *[_ptr(a, "field", 4) for a in (
+            inv_x, inv_y, inv_z, alpha_x, alpha_y, alpha_z, beta_x, beta_y, beta_z)],
+            volume, flow, nx, ny, nz, n_iter)
+
     def host_backprojection_adjoint(self, d_img, d_proj, angle, SO, SD, da, na, ai, db, nb, bi,
                                     nx, ny, nz):
         """Exact adjoint of host_projection (mcsart_backprojection_adjoint); no

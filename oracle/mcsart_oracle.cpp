@@ -305,6 +305,60 @@ void deform(T *out, const T *img, int nx, int ny, int nz, double volume, double 
             }
 }
 
+// Inverse of the warp's displacement for square slices (the engine's
+// mcsart_invert_dvf; not a reference function: the reference negates the
+// amplitudes, src/AUMISART.cu:222).  The warp samples memory position
+// q = (X, Y, Z) at q + D(q), D = (my, mx, mz)(q); N(q) = -D(q + N(q)) by
+// fixed-point iteration from 0 with exact trilinear samples, returned in the
+// forward layout (ox, oy, oz) = (N_Y, N_X, N_Z).
+template <typename T>
+void invert_dvf(T *ox, T *oy, T *oz, const T *ax, const T *ay, const T *az, const T *bx,
+                const T *by, const T *bz, double volume, double flow, int nx, int ny, int nz,
+                int iters) {
+    const int64_t n = nvox(nx, ny, nz);
+    std::vector<T> m(3 * n);
+    forward_dvf<T>(m.data(), m.data() + n, m.data() + 2 * n, ax, ay, az, bx, by, bz, volume,
+                   flow, nx, ny, nz);
+    const T *mx = m.data(), *my = mx + n, *mz = my + n;
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int Z = 0; Z < nz; Z++)
+        for (int Y = 0; Y < ny; Y++)
+            for (int X = 0; X < nx; X++) {
+                double NX = 0, NY = 0, NZ = 0;
+                for (int k = 0; k < iters; k++) {
+                    const double px = X + 0.5 + NX, py = Y + 0.5 + NY, pz = Z + 0.5 + NZ;
+                    const double dX = tex3d_linear<T>(my, nx, ny, nz, px, py, pz, ORC_TEX_EXACT);
+                    const double dY = tex3d_linear<T>(mx, nx, ny, nz, px, py, pz, ORC_TEX_EXACT);
+                    const double dZ = tex3d_linear<T>(mz, nx, ny, nz, px, py, pz, ORC_TEX_EXACT);
+                    NX = -dX;
+                    NY = -dY;
+                    NZ = -dZ;
+                }
+                const int64_t id = X + (int64_t)Y * nx + (int64_t)Z * nx * ny;
+                ox[id] = (T)NY;
+                oy[id] = (T)NX;
+                oz[id] = (T)NZ;
+            }
+}
+
+// The warp of src/cu_deform.cu:79-90 with an explicit displacement (mx, my,
+// mz) in place of alpha*volume + beta*flow, exact trilinear samples.
+template <typename T>
+void deform_disp(T *out, const T *img, int nx, int ny, int nz, const T *mx, const T *my,
+                 const T *mz) {
+    const int64_t n = nvox(nx, ny, nz);
+    std::vector<T> src(img, img + n);
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int iz = 0; iz < nz; iz++)
+        for (int ix = 0; ix < nx; ix++)
+            for (int iy = 0; iy < ny; iy++) {
+                const int64_t id = iy + (int64_t)ix * ny + (int64_t)iz * nx * ny;
+                out[id] = tex3d_linear<T>(src.data(), nx, ny, nz, iy + 0.5 + (double)my[id],
+                                          ix + 0.5 + (double)mx[id], iz + 0.5 + (double)mz[id],
+                                          ORC_TEX_EXACT);
+            }
+}
+
 // src/cu_deform.cu:49-64,92-113 (first-order warp).  With the transposed index
 // the +nx neighbour of the last x-row of the last slice lies past the end of
 // the volume in the reference (an out-of-bounds read there); it reads 0 here.
@@ -472,7 +526,7 @@ int aumisart(T *outimg, T *outproj, T *outnorm, T *outalphax, const T *h_img, co
              double /*dx*/, double lambda, const float *volumes, const float *flows,
              const float *angles, const T *fax, const T *fay, const T *faz, const T *fbx,
              const T *fby, const T *fbz, T *fields_out, int tex_mode, int view_lo, int view_hi,
-             int subset) {
+             int subset, int dvf_inverse) {
     const int64_t nv = nvox(nx, ny, nz), np = (int64_t)na * nb;
     const bool with_motion = fax != nullptr;  // overload 2
     if (view_hi < 0 || view_hi > n_views) view_hi = n_views;
@@ -533,7 +587,15 @@ int aumisart(T *outimg, T *outproj, T *outnorm, T *outalphax, const T *h_img, co
                 FP(proj_ones.data(), img_ones.data(), iv);
                 BP(img_ones.data(), proj_ones.data(), iv);
                 division<T>(img_temp.data(), img_ones.data(), nx, ny, nz);
-                if (with_motion) {
+                if (with_motion && dvf_inverse > 0) {  // the engine's options.dvf_inverse
+                    std::vector<T> inv(3 * nv);
+                    invert_dvf<T>(inv.data(), inv.data() + nv, inv.data() + 2 * nv, al_x, al_y,
+                                  al_z, be_x, be_y, be_z, volumes[iv] - volumes[0],
+                                  flows[iv] - flows[0], nx, ny, nz, dvf_inverse);
+                    deform_disp<T>(img1.data(), img_temp.data(), nx, ny, nz, inv.data(),
+                                   inv.data() + nv, inv.data() + 2 * nv);
+                    add<T>(img.data(), img1.data(), nx, ny, nz, lam);
+                } else if (with_motion) {
                     DEF(img1.data(), img_temp.data(), volumes[0] - volumes[iv],
                         flows[0] - flows[iv]);
                     add<T>(img.data(), img1.data(), nx, ny, nz, lam);
@@ -667,11 +729,17 @@ int aumisart(T *outimg, T *outproj, T *outnorm, T *outalphax, const T *h_img, co
         const int *op_iter, double da, double db, double ai, double bi, double SO, double SD,  \
         double dx, double lambda, const float *volumes, const float *flows,                    \
         const float *angles, const T *ax, const T *ay, const T *az, const T *bx, const T *by,  \
-        const T *bz, T *fields_out, int tex_mode, int view_lo, int view_hi, int subset) {      \
+        const T *bz, T *fields_out, int tex_mode, int view_lo, int view_hi, int subset,        \
+        int dvf_inverse) {                                                                     \
         return aumisart<T>(outimg, outproj, outnorm, outalphax, img, proj, nx, ny, nz, na, nb, \
                            outIter, n_views, n_iter, op_iter, da, db, ai, bi, SO, SD, dx,      \
                            lambda, volumes, flows, angles, ax, ay, az, bx, by, bz, fields_out, \
-                           tex_mode, view_lo, view_hi, subset);                                \
+                           tex_mode, view_lo, view_hi, subset, dvf_inverse);                   \
+    }                                                                                          \
+    extern "C" void P##invert_dvf(T *ox, T *oy, T *oz, const T *ax, const T *ay, const T *az,  \
+                                  const T *bx, const T *by, const T *bz, double volume,        \
+                                  double flow, int nx, int ny, int nz, int iters) {            \
+        invert_dvf<T>(ox, oy, oz, ax, ay, az, bx, by, bz, volume, flow, nx, ny, nz, iters);    \
     }
 
 ORC_DEFINE(double, orc_)

@@ -60,7 +60,10 @@ enum { ORC_TEX_EXACT = 0, ORC_TEX_Q8_NEAREST = 1, ORC_TEX_Q8_TRUNC = 2 };
                     const float *volumes, const float *flows, const float *angles,             \
                     const T *ax, const T *ay, const T *az, const T *bx, const T *by,           \
                     const T *bz, T *fields_out, int tex_mode, int view_lo, int view_hi,       \
-                    int subset);
+                    int subset, int dvf_inverse);                                             \
+    void P##invert_dvf(T *ox, T *oy, T *oz, const T *ax, const T *ay, const T *az, const T *bx, \
+                       const T *by, const T *bz, double volume, double flow, int nx, int ny,  \
+                       int nz, int iters);
 
 ORC_DECL(double, orc_)
 ORC_DECL(float, cpu_)

@@ -66,7 +66,9 @@ def _declare(L: ctypes.CDLL) -> None:
         getattr(L, pre + "update_udvf").argtypes = [_P] * 8 + [_D, _D, _I, _I, _I, _I]
         getattr(L, pre + "diff").argtypes = [_P, _P, _I, _I, _I, _I]
         f = getattr(L, pre + "aumisart")
-        f.argtypes = ([_P] * 6 + [_I] * 8 + [_P] + [_D] * 8 + [_P] * 3 + [_P] * 6 + [_P, _I, _I, _I, _I])
+        f.argtypes = ([_P] * 6 + [_I] * 8 + [_P] + [_D] * 8 + [_P] * 3 + [_P] * 6 +
+                      [_P, _I, _I, _I, _I, _I])
+        getattr(L, pre + "invert_dvf").argtypes = [_P] * 9 + [_D, _D, _I, _I, _I, _I]
         f.restype = _I
     L.orc_num_threads.restype = _I
     L.orc_set_num_threads.argtypes = [_I]
@@ -112,6 +114,17 @@ def backprojection(proj, angle, geo, prec="orc"):
     proj = _arr(proj, prec)
     out = np.zeros((geo["nz"], geo["ny"], geo["nx"]), _dt(prec))
     getattr(lib(), prec + "_backprojection")(_p(out), _p(proj), float(angle), *_geo(geo))
+    return out
+
+
+def invert_dvf(fields, volume, flow, iters, prec="orc"):
+    """Fixed-point inverse of the warp's displacement (the engine's
+    mcsart_invert_dvf); returns (inv_x, inv_y, inv_z)."""
+    f = [_arr(x, prec) for x in fields]
+    nz, ny, nx = f[0].shape
+    out = [np.zeros_like(f[0]) for _ in range(3)]
+    getattr(lib(), prec + "_invert_dvf")(*[_p(x) for x in out], *[_p(x) for x in f],
+                                        float(volume), float(flow), nx, ny, nz, int(iters))
     return out
 
 
@@ -236,7 +249,7 @@ def diff(img, ind, prec="orc", init=None):
 
 
 def aumisart(img, proj, geo, it, fields=None, tex_mode=TEX_Q8_NEAREST, prec="orc",
-             view_lo=0, view_hi=-1, return_fields=False, subset=1):
+             view_lo=0, view_hi=-1, return_fields=False, subset=1, dvf_inverse=0):
     """The SART/motion loop of host_AUMISART (src/AUMISART.cu:3 and :143).
 
     ``it`` holds ``n_iter``, ``op_iter``, ``n_views``, ``lambda``, ``volumes``,
@@ -268,7 +281,7 @@ def aumisart(img, proj, geo, it, fields=None, tex_mode=TEX_Q8_NEAREST, prec="orc
         float(geo["db"]), float(geo["ai"]), float(geo["bi"]), float(geo["SO"]),
         float(geo["SD"]), float(geo.get("dx", 1.0)), float(it["lambda"]), _p(vols), _p(flows),
         _p(angs), *[_p(x) for x in f], _p(fo), int(tex_mode), int(view_lo), int(view_hi),
-        int(subset))
+        int(subset), int(dvf_inverse))
     if rc != 0:
         raise RuntimeError(f"oracle aumisart failed: {rc}")
     out = {"img": out_img, "norm": out_norm, "alpha_x": out_ax, "resid": out_proj}
