@@ -134,6 +134,28 @@ __device__ __forceinline__ bool mk_num_ok(float a) {
     return __float_as_uint(a) == 0u || (m >= 0x1p-80f && m <= 0x1p80f);
 }
 
+// floor to int and int to float on the FMA and integer pipes instead of the
+// conversion unit (which the projector otherwise keeps busy), exact for
+// |x| < 2^22: the floats in [2^23, 2^24) are the integers, so x + 1.5*2^23
+// rounded toward -inf is 1.5*2^23 + floor(x), whose low significand bits are
+// floor(x) + 2^22 (the magic-number conversion).  Callers keep their
+// arguments inside the range.
+constexpr float MK_MAGIC = 12582912.0f;  // 1.5 * 2^23
+constexpr int MK_MAGIC_BITS = 0x4B400000;
+constexpr float MK_MAGIC_RANGE = 4194304.0f;  // 2^22
+__device__ __forceinline__ int mk_floor_i(float x) {
+    return __float_as_int(__fadd_rd(x, MK_MAGIC)) - MK_MAGIC_BITS;
+}
+// floor(x) as an int and as a float
+__device__ __forceinline__ int mk_floor(float x, float &fl) {
+    const float t = __fadd_rd(x, MK_MAGIC);
+    fl = __fsub_rn(t, MK_MAGIC);
+    return __float_as_int(t) - MK_MAGIC_BITS;
+}
+__device__ __forceinline__ float mk_i2f(int i) {
+    return __fsub_rn(__int_as_float(MK_MAGIC_BITS + i), MK_MAGIC);
+}
+
 __host__ __device__ inline int64_t nvox(int nx, int ny, int nz) { return (int64_t)nx * ny * nz; }
 
 int validate_geom(const Geom &g);

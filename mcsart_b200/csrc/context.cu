@@ -81,6 +81,11 @@ int validate_geom(const Geom &g) {
     MC_REQUIRE(g.na > 0 && g.nb > 0, "detector dimensions must be positive (got %d x %d)", g.na,
                g.nb);
     MC_REQUIRE((int64_t)g.na * g.nb < (int64_t)1 << 31, "detector too large");
+    // the projector converts slab indices with the magic-number conversion,
+    // exact below 2^22
+    const int lim = 1 << 20;
+    MC_REQUIRE(g.nx <= lim && g.ny <= lim && g.nz <= lim && g.na <= lim && g.nb <= lim,
+               "volume and detector dimensions must be at most 2^20");
     MC_REQUIRE(g.SO > 0.0f && g.SD > 0.0f, "SO and SD must be positive");
     MC_REQUIRE(g.da > 0.0f && g.db > 0.0f, "detector pitches da, db must be positive");
     return MCSART_OK;

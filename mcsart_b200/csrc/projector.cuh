@@ -258,8 +258,9 @@ template <typename VT, int K, typename MT = VT> struct FPArgs {
 // driving axis, the four edge ratios and so, per slab, the in-plane voxel
 // range U1..U2 and weights w_u (only the axial part depends on the row ib,
 // through z2).  A block of FPC_COLS columns x FPC_ROWS rows computes the
-// in-plane part once per (column, slab) into shared memory, FPC_CHUNK slabs
-// at a time, and every ray then adds its axial part and its terms in the
+// in-plane part once per (column, slab) into shared memory (SlabC: weights,
+// slab distance, clamped voxel-row offsets, visit flags), FPC_CHUNK slabs at
+// a time, and every ray then adds its axial part and its terms in the
 // reference's order.  The per-ray arithmetic is unchanged, so the sums are
 // bitwise those of the per-ray form (and of the reference kernel).
 #ifndef MCSART_FP_COLS
@@ -286,9 +287,15 @@ struct SlabU {
     float a, b;
 };
 
+// :52 / :105: distance of slab d's centre from the source along the driving
+// axis (d < 2^20, validate_geom: mk_i2f is exact).
+__device__ __forceinline__ float slab_dc(const RayGeom &r, int d) {
+    return __fsub_rn(__fsub_rn(__fadd_rn(mk_i2f(d), 0.5f), r.d_half), r.src_d);
+}
+
 // :52-63 / :105-116 for slab d of the ray's column.
 __device__ __forceinline__ SlabU slab_u(const RayGeom &r, int d) {
-    const float dc = __fsub_rn(__fsub_rn(__fadd_rn((float)d, 0.5f), r.d_half), r.src_d);
+    const float dc = slab_dc(r, d);
     const float c0 = __fadd_rn(__fmaf_rn(r.r0, dc, r.u_off), r.u_half);
     const float c1 = __fadd_rn(__fmaf_rn(r.r1, dc, r.u_off), r.u_half);
     const float c2 = __fadd_rn(__fmaf_rn(r.r2, dc, r.u_off), r.u_half);
@@ -296,11 +303,19 @@ __device__ __forceinline__ SlabU slab_u(const RayGeom &r, int d) {
     const float ui1 = fminf(fminf(c0, c1), fminf(c2, c3));
     const float ui2 = fmaxf(fmaxf(c0, c1), fmaxf(c2, c3));
     SlabU e;
-    e.U1 = (int)floorf(ui1);
-    e.U2 = (int)floorf(ui2);
+    float fu0, fu1;
+    if (fabsf(ui1) < MK_MAGIC_RANGE && fabsf(ui2) < MK_MAGIC_RANGE) {
+        e.U1 = mk_floor(ui1, fu0);
+        e.U2 = mk_floor_i(ui2);
+        fu1 = __fadd_rn(fu0, 1.0f);  // (float)(U1 + 1), exact below 2^22
+    } else {
+        e.U1 = (int)floorf(ui1);
+        e.U2 = (int)floorf(ui2);
+        fu0 = (float)e.U1;
+        fu1 = (float)(e.U1 + 1);
+    }
     if (e.U2 - e.U1 <= 1) {
         const float du = __fsub_rn(ui2, ui1);  // :83 / :136
-        const float fu0 = (float)e.U1, fu1 = (float)(e.U1 + 1);
         const float n0 = __fsub_rn(fminf(__fadd_rn(fu0, 1.0f), ui2), fmaxf(fu0, ui1));
         const float n1 = __fsub_rn(fminf(__fadd_rn(fu1, 1.0f), ui2), fmaxf(fu1, ui1));
         const float y = mk_recip(du);
@@ -317,6 +332,37 @@ __device__ __forceinline__ SlabU slab_u(const RayGeom &r, int d) {
     return e;
 }
 
+// What every ray of one detector column shares for slab d, kept in shared
+// memory: slab_u's footprint, the slab distance dc, the clamped offsets of
+// the window's two in-plane voxel rows (cu * su + d * sd) and which of the two
+// the reference's loops visit (:80-82 / :133-135).
+struct __align__(16) SlabC {
+    int r0, r1;
+    float a, b;  // SlabU's
+    float dc;
+    int U1, U2;
+    int flags;   // SC_U0 | SC_U1 | SC_NARROW (U2 - U1 <= 1)
+};
+constexpr int SC_U0 = 1, SC_U1 = 2, SC_NARROW = 4;
+
+__device__ __forceinline__ SlabC slab_c(const RayGeom &r, int d, int su, int sd) {
+    const SlabU e = slab_u(r, d);
+    SlabC c;
+    c.a = e.a;
+    c.b = e.b;
+    c.U1 = e.U1;
+    c.U2 = e.U2;
+    c.dc = slab_dc(r, d);
+    const int U1 = e.U1, U2 = e.U2;
+    const bool u0 = U1 >= 0 && U1 <= r.nu - 1;
+    const bool u1 = U1 + 1 <= U2 && U1 + 1 >= 0 && U1 + 1 <= r.nu - 1;
+    c.flags = (u0 ? SC_U0 : 0) | (u1 ? SC_U1 : 0) | (U2 - U1 <= 1 ? SC_NARROW : 0);
+    const int cu0 = min(max(U1, 0), r.nu - 1), cu1 = min(max(U1 + 1, 0), r.nu - 1);
+    c.r0 = cu0 * su + d * sd;
+    c.r1 = cu1 * su + d * sd;
+    return c;
+}
+
 // A 2x2 footprint window (U1, U1+1) x (Z1, Z1+1) of one slab: weights,
 // clamped (always in-bounds) addresses and which of the four voxels the
 // reference's loops visit (:80-88 / :133-141).
@@ -327,54 +373,62 @@ struct SlabZ {
 };
 
 // Axial part of slab d for this ray; true (and w filled) if the footprint is
-// a 2x2 window whose weights the branch-free division computed exactly.  Voxel indices are 32-bit: volumes are validated to hold
-// fewer than 2^31 voxels (the reference indexes with int as well).
-__device__ __forceinline__ bool slab_window(const RayGeom &r, const Geom &g, const SlabU &e, int d,
-                                            int su, int sd, int sz, float z_half, SlabZ &w) {
-    const float dc = __fsub_rn(__fsub_rn(__fadd_rn((float)d, 0.5f), r.d_half), r.src_d);
+// a 2x2 window whose weights the branch-free division computed exactly.
+// zsafe: the ray's axial coordinates stay below 2^22 in magnitude, where the
+// magic-number floor is exact (otherwise the caller takes the general path).
+// Voxel indices are 32-bit: volumes are validated to hold fewer than 2^31
+// voxels (the reference indexes with int as well).
+__device__ __forceinline__ bool slab_window(const RayGeom &r, const Geom &g, const SlabC &c, int sz,
+                                            float z_half, bool zsafe, SlabZ &w) {
     // :71-77 / :124-130 ("ratio * xc + z1 + nz / 2", z1 = 0)
-    const float cz0 = __fadd_rn(__fmul_rn(r.rz0, dc), z_half);
-    const float cz1 = __fadd_rn(__fmul_rn(r.rz1, dc), z_half);
+    const float cz0 = __fadd_rn(__fmul_rn(r.rz0, c.dc), z_half);
+    const float cz1 = __fadd_rn(__fmul_rn(r.rz1, c.dc), z_half);
     const float zi1 = fminf(cz0, cz1), zi2 = fmaxf(cz0, cz1);
-    const int Z1 = (int)floorf(zi1), Z2 = (int)floorf(zi2);
+    float fz0;
+    const int Z1 = mk_floor(zi1, fz0), Z2 = mk_floor_i(zi2);
+    const float fz1 = __fadd_rn(fz0, 1.0f);
     const float dz = __fsub_rn(zi2, zi1);
-    const int U1 = e.U1, U2 = e.U2;
-    const bool u0 = U1 >= 0 && U1 <= r.nu - 1;
-    const bool u1 = U1 + 1 <= U2 && U1 + 1 >= 0 && U1 + 1 <= r.nu - 1;
+    const bool u0 = c.flags & SC_U0, u1 = c.flags & SC_U1;
     const bool z0 = Z1 >= 0 && Z1 <= g.nz - 1;
     const bool z1 = Z1 + 1 <= Z2 && Z1 + 1 >= 0 && Z1 + 1 <= g.nz - 1;
     w.p00 = u0 && z0;
     w.p01 = u0 && z1;
     w.p10 = u1 && z0;
     w.p11 = u1 && z1;
-    w.wu0 = e.a;
-    w.wu1 = e.b;
-    const float fz0 = (float)Z1, fz1 = (float)(Z1 + 1);
-    const float n0 = __fsub_rn(fminf(__fadd_rn(fz0, 1.0f), zi2), fmaxf(fz0, zi1));
+    w.wu0 = c.a;
+    w.wu1 = c.b;
+    const float n0 = __fsub_rn(fminf(fz1, zi2), fmaxf(fz0, zi1));
     const float n1 = __fsub_rn(fminf(__fadd_rn(fz1, 1.0f), zi2), fmaxf(fz1, zi1));
     const float y = mk_recip(dz);
     w.wz0 = mk_div(n0, dz, y);
     w.wz1 = mk_div(n1, dz, y);
     const bool exact = mk_den_ok(dz) && mk_num_ok(n0) && mk_num_ok(n1);
-    const int cu0 = min(max(U1, 0), r.nu - 1), cu1 = min(max(U1 + 1, 0), r.nu - 1);
     const int cz0i = min(max(Z1, 0), g.nz - 1), cz1i = min(max(Z1 + 1, 0), g.nz - 1);
-    const int r0 = cu0 * su + d * sd, r1 = cu1 * su + d * sd;
-    w.a00 = r0 + cz0i * sz;
-    w.a01 = r0 + cz1i * sz;
-    w.a10 = r1 + cz0i * sz;
-    w.a11 = r1 + cz1i * sz;
+    w.a00 = c.r0 + cz0i * sz;
+    w.a01 = c.r0 + cz1i * sz;
+    w.a10 = c.r1 + cz0i * sz;
+    w.a11 = c.r1 + cz1i * sz;
     // outside the division's checked range the caller takes the general path
-    return U2 - U1 <= 1 && Z2 - Z1 <= 1 && exact;
+    return (c.flags & SC_NARROW) && Z2 - Z1 <= 1 && exact && zsafe;
+}
+
+// Whether every axial footprint coordinate of the ray, rz * dc + nz/2 over
+// its slabs, stays below 2^21 in magnitude (a factor 2 inside the range of
+// the magic-number floor, for rounding).
+__device__ __forceinline__ bool ray_zsafe(const RayGeom &r, float z_half) {
+    const float dmax = 1.5f * (float)r.nd + fabsf(r.src_d) + 2.0f;
+    const float zmax = fmaxf(fabsf(r.rz0), fabsf(r.rz1)) * dmax + fabsf(z_half) + 2.0f;
+    return zmax < 0.5f * MK_MAGIC_RANGE;
 }
 
 // One slab of one ray, any footprint: the 2x2 window with predication or the
 // reference's loops (:80-88 / :133-141).
 template <int K, bool ONES, typename VT>
-__device__ __forceinline__ void fp_slab(const RayGeom &r, const Geom &g, const SlabU &e, int d,
+__device__ __forceinline__ void fp_slab(const RayGeom &r, const Geom &g, const SlabC &e, int d,
                                         const VT *const *base, int su, int sd, int sz,
-                                        float z_half, float *acc, float &accw) {
+                                        float z_half, bool zsafe, float *acc, float &accw) {
     SlabZ w;
-    if (slab_window(r, g, e, d, su, sd, sz, z_half, w)) {
+    if (slab_window(r, g, e, sz, z_half, zsafe, w)) {
 #pragma unroll
         for (int k = 0; k < K; k++) {
             if (w.p00) acc[k] = __fmaf_rn(__fmul_rn(ldv(base[k], w.a00), w.wu0), w.wz0, acc[k]);
@@ -390,9 +444,8 @@ __device__ __forceinline__ void fp_slab(const RayGeom &r, const Geom &g, const S
         }
         return;
     }
-    const float dc = __fsub_rn(__fsub_rn(__fadd_rn((float)d, 0.5f), r.d_half), r.src_d);
-    const float cz0 = __fadd_rn(__fmul_rn(r.rz0, dc), z_half);
-    const float cz1 = __fadd_rn(__fmul_rn(r.rz1, dc), z_half);
+    const float cz0 = __fadd_rn(__fmul_rn(r.rz0, e.dc), z_half);
+    const float cz1 = __fadd_rn(__fmul_rn(r.rz1, e.dc), z_half);
     const float zi1 = fminf(cz0, cz1), zi2 = fmaxf(cz0, cz1);
     const int Z1 = (int)floorf(zi1), Z2 = (int)floorf(zi2);
     const float dz = __fsub_rn(zi2, zi1);
@@ -419,14 +472,101 @@ __device__ __forceinline__ void fp_slab(const RayGeom &r, const Geom &g, const S
     }
 }
 
+// The windows of slabs d0+j .. d0+j+FPC_GROUP-1 of a ray and the 4*K voxel
+// values of each (addresses are clamped, so every load is in bounds); true if
+// all of them are exact 2x2 windows.
+template <int K, typename VT>
+__device__ __forceinline__ bool fp_group_load(const RayGeom &r, const Geom &g,
+                                              const SlabC (*sm_c)[FPC_COLS], int col, int j, int sz,
+                                              const VT *const *base, float z_half, bool zsafe,
+                                              SlabZ *w,
+                                              float (*v)[K][4]) {
+    bool all_fast = true;
+#pragma unroll
+    for (int q = 0; q < FPC_GROUP; q++)
+        all_fast &= slab_window(r, g, sm_c[j + q][col], sz, z_half, zsafe, w[q]);
+#pragma unroll
+    for (int q = 0; q < FPC_GROUP; q++)
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            v[q][k][0] = ldv(base[k], w[q].a00);
+            v[q][k][1] = ldv(base[k], w[q].a01);
+            v[q][k][2] = ldv(base[k], w[q].a10);
+            v[q][k][3] = ldv(base[k], w[q].a11);
+        }
+    return all_fast;
+}
+
+// The terms of one group in the reference's order: from the loaded windows
+// when all are 2x2 (fast), else slab by slab on the general path.
+template <int K, bool ONES, typename VT>
+__device__ __forceinline__ void fp_group_sum(const RayGeom &r, const Geom &g,
+                                             const SlabC (*sm_c)[FPC_COLS], int col, int j, int d0,
+                                             const VT *const *base, int su, int sd, int sz,
+                                             float z_half, bool zsafe, bool fast, const SlabZ *w,
+                                             const float (*v)[K][4], float *acc, float &accw) {
+    if (!fast) {
+#pragma unroll 1
+        for (int q = 0; q < FPC_GROUP; q++)
+            fp_slab<K, ONES, VT>(r, g, sm_c[j + q][col], d0 + j + q, base, su, sd, sz, z_half, zsafe,
+                                 acc, accw);
+        return;
+    }
+#pragma unroll
+    for (int q = 0; q < FPC_GROUP; q++) {
+        const SlabZ &x = w[q];
+        if (K == 1 && ONES) {
+            // one volume and the weight sum: the two chains interleaved term
+            // by term (measured faster here; the per-volume order below is
+            // faster with three volumes)
+            if (x.p00) {
+                acc[0] = __fmaf_rn(__fmul_rn(v[q][0][0], x.wu0), x.wz0, acc[0]);
+                accw = __fmaf_rn(x.wu0, x.wz0, accw);
+            }
+            if (x.p01) {
+                acc[0] = __fmaf_rn(__fmul_rn(v[q][0][1], x.wu0), x.wz1, acc[0]);
+                accw = __fmaf_rn(x.wu0, x.wz1, accw);
+            }
+            if (x.p10) {
+                acc[0] = __fmaf_rn(__fmul_rn(v[q][0][2], x.wu1), x.wz0, acc[0]);
+                accw = __fmaf_rn(x.wu1, x.wz0, accw);
+            }
+            if (x.p11) {
+                acc[0] = __fmaf_rn(__fmul_rn(v[q][0][3], x.wu1), x.wz1, acc[0]);
+                accw = __fmaf_rn(x.wu1, x.wz1, accw);
+            }
+            continue;
+        }
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            if (x.p00) acc[k] = __fmaf_rn(__fmul_rn(v[q][k][0], x.wu0), x.wz0, acc[k]);
+            if (x.p01) acc[k] = __fmaf_rn(__fmul_rn(v[q][k][1], x.wu0), x.wz1, acc[k]);
+            if (x.p10) acc[k] = __fmaf_rn(__fmul_rn(v[q][k][2], x.wu1), x.wz0, acc[k]);
+            if (x.p11) acc[k] = __fmaf_rn(__fmul_rn(v[q][k][3], x.wu1), x.wz1, acc[k]);
+        }
+        if (ONES) {
+            if (x.p00) accw = __fmaf_rn(x.wu0, x.wz0, accw);
+            if (x.p01) accw = __fmaf_rn(x.wu0, x.wz1, accw);
+            if (x.p10) accw = __fmaf_rn(x.wu1, x.wz0, accw);
+            if (x.p11) accw = __fmaf_rn(x.wu1, x.wz1, accw);
+        }
+    }
+}
+
 // blockDim = FPC_THREADS: thread t is column t % FPC_COLS, row t / FPC_COLS;
 // gridDim = (ceil(na/FPC_COLS), ceil(nb/FPC_ROWS), views).
 // MULTI = true: several views per launch (ordered subsets, kernel-level
 // multi-view projection), view = blockIdx.z with the per-view offsets of
 // FPArgs; false: one view per launch without them.
+// Resident blocks per SM the register budget must allow: one volume, 6 (at
+// most 80 registers, which the kernel fits without spilling); three volumes,
+// FPC_MIN_BLOCKS.  Large detectors fill every SM, and there the one-volume
+// projector runs 6 blocks per SM instead of 5 (4.6 % less projector time at
+// 512x384 rays per view; unchanged at 256x192, where fewer blocks exist).
+constexpr int FPC_MIN_BLOCKS_K1 = 6;
 template <int K, bool ONES, typename VT, typename MT = VT, bool MULTI = false>
-__global__ void __launch_bounds__(FPC_THREADS, FPC_MIN_BLOCKS) fp_ref_kernel(const FPArgs<VT, K, MT> p) {
-    __shared__ SlabU sm_u[FPC_CHUNK][FPC_COLS];
+__global__ void __launch_bounds__(FPC_THREADS, K == 1 ? FPC_MIN_BLOCKS_K1 : FPC_MIN_BLOCKS) fp_ref_kernel(const FPArgs<VT, K, MT> p) {
+    __shared__ SlabC sm_c[FPC_CHUNK][FPC_COLS];
     __shared__ double2 sm_norm[FPC_THREADS / 32];
     const Geom &g = p.g;
     const int t = threadIdx.x, col = t % FPC_COLS, row = t / FPC_COLS;
@@ -462,87 +602,36 @@ __global__ void __launch_bounds__(FPC_THREADS, FPC_MIN_BLOCKS) fp_ref_kernel(con
 #pragma unroll
     for (int k = 0; k < K; k++) acc[k] = 0.0f;
 
+    const bool zsafe = ray_zsafe(r, z_half);
     const int nd_max = max(g.nx, g.ny);
     for (int d0 = 0; d0 < nd_max; d0 += FPC_CHUNK) {
         for (int j = row; j < FPC_CHUNK; j += FPC_ROWS) {
             const int d = d0 + j;
-            SlabU e;
-            e.U1 = 0; e.U2 = -1; e.a = 0.0f; e.b = 0.0f;
-            if (col_ok && d < r.nd) e = slab_u(r, d);
-            sm_u[j][col] = e;
+            SlabC e;
+            e.r0 = 0; e.r1 = 0; e.a = 0.0f; e.b = 0.0f; e.dc = 0.0f;
+            e.U1 = 0; e.U2 = -1; e.flags = 0;
+            if (col_ok && d < r.nd) e = slab_c(r, d, su, sd);
+            sm_c[j][col] = e;
         }
         __syncthreads();
         const int dn = active ? min(FPC_CHUNK, r.nd - d0) : 0;
-        int j = 0;
-        // groups of FPC_GROUP slabs whose footprints are all 2x2 windows: the
-        // set-up and the (always in-bounds) loads of the whole group come
-        // first, then the terms enter the sums in the reference's order, so
-        // that a warp waits for memory once per group instead of per slab
-        for (; j + FPC_GROUP <= dn; j += FPC_GROUP) {
+        // Groups of FPC_GROUP slabs: the windows and the (always in-bounds)
+        // loads of a whole group are issued together before its terms enter
+        // the sums in the reference's order, so that a warp waits for memory
+        // once per group instead of per slab.  A group whose footprints are
+        // not all 2x2 windows takes the general per-slab path.
+        const int ng = dn / FPC_GROUP;
+        for (int i = 0; i < ng; i++) {
             SlabZ w[FPC_GROUP];
-            bool all_fast = true;
-#pragma unroll
-            for (int q = 0; q < FPC_GROUP; q++)
-                all_fast &= slab_window(r, g, sm_u[j + q][col], d0 + j + q, su, sd, sz, z_half, w[q]);
-            if (all_fast) {
-                float v[FPC_GROUP][K][4];
-#pragma unroll
-                for (int q = 0; q < FPC_GROUP; q++)
-#pragma unroll
-                    for (int k = 0; k < K; k++) {
-                        v[q][k][0] = ldv(base[k], w[q].a00);
-                        v[q][k][1] = ldv(base[k], w[q].a01);
-                        v[q][k][2] = ldv(base[k], w[q].a10);
-                        v[q][k][3] = ldv(base[k], w[q].a11);
-                    }
-#pragma unroll
-                for (int q = 0; q < FPC_GROUP; q++) {
-                    const SlabZ &x = w[q];
-                    if (K == 1 && ONES) {
-                        // one volume and the weight sum: the two chains
-                        // interleaved term by term (measured faster here; the
-                        // per-volume order below is faster with three volumes)
-                        if (x.p00) {
-                            acc[0] = __fmaf_rn(__fmul_rn(v[q][0][0], x.wu0), x.wz0, acc[0]);
-                            accw = __fmaf_rn(x.wu0, x.wz0, accw);
-                        }
-                        if (x.p01) {
-                            acc[0] = __fmaf_rn(__fmul_rn(v[q][0][1], x.wu0), x.wz1, acc[0]);
-                            accw = __fmaf_rn(x.wu0, x.wz1, accw);
-                        }
-                        if (x.p10) {
-                            acc[0] = __fmaf_rn(__fmul_rn(v[q][0][2], x.wu1), x.wz0, acc[0]);
-                            accw = __fmaf_rn(x.wu1, x.wz0, accw);
-                        }
-                        if (x.p11) {
-                            acc[0] = __fmaf_rn(__fmul_rn(v[q][0][3], x.wu1), x.wz1, acc[0]);
-                            accw = __fmaf_rn(x.wu1, x.wz1, accw);
-                        }
-                        continue;
-                    }
-#pragma unroll
-                    for (int k = 0; k < K; k++) {
-                        if (x.p00) acc[k] = __fmaf_rn(__fmul_rn(v[q][k][0], x.wu0), x.wz0, acc[k]);
-                        if (x.p01) acc[k] = __fmaf_rn(__fmul_rn(v[q][k][1], x.wu0), x.wz1, acc[k]);
-                        if (x.p10) acc[k] = __fmaf_rn(__fmul_rn(v[q][k][2], x.wu1), x.wz0, acc[k]);
-                        if (x.p11) acc[k] = __fmaf_rn(__fmul_rn(v[q][k][3], x.wu1), x.wz1, acc[k]);
-                    }
-                    if (ONES) {
-                        if (x.p00) accw = __fmaf_rn(x.wu0, x.wz0, accw);
-                        if (x.p01) accw = __fmaf_rn(x.wu0, x.wz1, accw);
-                        if (x.p10) accw = __fmaf_rn(x.wu1, x.wz0, accw);
-                        if (x.p11) accw = __fmaf_rn(x.wu1, x.wz1, accw);
-                    }
-                }
-            } else {
-#pragma unroll 1
-                for (int q = 0; q < FPC_GROUP; q++)
-                    fp_slab<K, ONES, VT>(r, g, sm_u[j + q][col], d0 + j + q, base, su, sd, sz, z_half,
-                                         acc, accw);
-            }
+            float v[FPC_GROUP][K][4];
+            const bool fast = fp_group_load<K>(r, g, sm_c, col, i * FPC_GROUP, sz, base, z_half,
+                                               zsafe, w, v);
+            fp_group_sum<K, ONES, VT>(r, g, sm_c, col, i * FPC_GROUP, d0, base, su, sd, sz, z_half,
+                                      zsafe, fast, w, v, acc, accw);
         }
-        for (; j < dn; j++)
-            fp_slab<K, ONES, VT>(r, g, sm_u[j][col], d0 + j, base, su, sd, sz, z_half, acc, accw);
+        for (int j = ng * FPC_GROUP; j < dn; j++)
+            fp_slab<K, ONES, VT>(r, g, sm_c[j][col], d0 + j, base, su, sd, sz, z_half, zsafe, acc,
+                                 accw);
         __syncthreads();
     }
 

@@ -2,7 +2,10 @@
 // mcsart_b200/csrc/common.cuh) bit for bit against the compiler's correctly
 // rounded reciprocal and division: every significand of the divisor for
 // exponents -20 .. 19, and random quotients (projector-weight operands and
-// operands over 2^-20 .. 2^20).  Prints four mismatch counts.
+// operands over 2^-20 .. 2^20); and the magic-number conversions (mk_floor,
+// mk_floor_i, mk_i2f) against floorf and int-to-float for
+// every float of magnitude below 2^22 and every int in [-2^22, 2^22).  Prints
+// five mismatch counts.
 #include <cstdio>
 
 #include "common.cuh"
@@ -56,15 +59,38 @@ __global__ void check_random(unsigned long long *bad, uint32_t seed, int n_per) 
     }
 }
 
+// blockIdx.y = sign * 256 + biased exponent (0 .. 148: |x| < 2^22)
+__global__ void check_conversions(unsigned long long *bad) {
+    const uint32_t m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= (1u << 23)) return;
+    const uint32_t e = blockIdx.y & 255u, s = blockIdx.y >> 8;
+    const float x = __uint_as_float((s << 31) | (e << 23) | m);
+    if (!(fabsf(x) < MK_MAGIC_RANGE)) return;
+    float fl;
+    const int i = mk_floor(x, fl);
+    const float rf = floorf(x);
+    int n = 0;
+    n += i != (int)rf;
+    n += mk_floor_i(x) != (int)rf;
+    n += __float_as_uint(fl) != __float_as_uint((float)(int)rf);  // a zero floor is +0
+    if (e == 0) {  // every int of [-2^22, 2^22) once, from the e = 0 blocks
+        const int k = (int)m - (s ? (1 << 23) : 0);  // [-2^23, 2^23)
+        if (k >= -(1 << 22) && k < (1 << 22))
+            n += __float_as_uint(mk_i2f(k)) != __float_as_uint((float)k);
+    }
+    if (n) atomicAdd(&bad[4], (unsigned long long)n);
+}
+
 int main() {
-    unsigned long long *bad = nullptr, h[4] = {0, 0, 0, 0};
+    unsigned long long *bad = nullptr, h[5] = {0, 0, 0, 0, 0};
     if (cudaMalloc(&bad, sizeof(h)) != cudaSuccess) return 2;
     cudaMemset(bad, 0, sizeof(h));
     check_exhaustive<<<dim3((1u << 23) / 256, 40), 256>>>(bad, -20);
     for (int s = 0; s < 2; s++) check_random<<<148 * 16, 256>>>(bad, 77u + s, 1024);
+    check_conversions<<<dim3((1u << 23) / 256, 512), 256>>>(bad);
     if (cudaDeviceSynchronize() != cudaSuccess) return 3;
     cudaMemcpy(h, bad, sizeof(h), cudaMemcpyDeviceToHost);
     cudaFree(bad);
-    printf("%llu %llu %llu %llu\n", h[0], h[1], h[2], h[3]);
+    printf("%llu %llu %llu %llu %llu\n", h[0], h[1], h[2], h[3], h[4]);
     return 0;
 }
