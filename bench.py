@@ -164,8 +164,8 @@ def algorithmic_bytes(p) -> dict:
 # c2 workload's kernels, from one `ncu --set full` capture of each (cold cache,
 # FP32 storage); summaries with the commands are kept under profiles/.
 NCU_DRAM_BYTES_C2 = {
-    "fp_motion": 15439360 + 0,
-    "fp_image": 5301248 + 0,
+    "fp_motion": 15459328 + 0,
+    "fp_image": 5316864 + 0,
     "bp_div": 409856 + 0,
     "field_update_prep": 50349824 + 5771264,
 }
@@ -174,7 +174,7 @@ NCU_DRAM_BYTES_C2 = {
 # Issue-slot utilisation (smsp__issue_active) of the projector and
 # backprojector from the same captures: these kernels are bound by issue and
 # latency, not by HBM.
-NCU_ISSUE_ACTIVE_C2 = {"fp_image": 0.417, "fp_motion": 0.429, "bp_div": 0.764}
+NCU_ISSUE_ACTIVE_C2 = {"fp_image": 0.428, "fp_motion": 0.435, "bp_div": 0.764}
 
 
 def measured_peaks() -> dict:

@@ -143,14 +143,15 @@ __device__ __forceinline__ bool mk_num_ok(float a) {
 constexpr float MK_MAGIC = 12582912.0f;  // 1.5 * 2^23
 constexpr int MK_MAGIC_BITS = 0x4B400000;
 constexpr float MK_MAGIC_RANGE = 4194304.0f;  // 2^22
+// (the subtraction is unsigned: out of range it wraps instead of overflowing)
 __device__ __forceinline__ int mk_floor_i(float x) {
-    return __float_as_int(__fadd_rd(x, MK_MAGIC)) - MK_MAGIC_BITS;
+    return (int)(__float_as_uint(__fadd_rd(x, MK_MAGIC)) - (unsigned)MK_MAGIC_BITS);
 }
 // floor(x) as an int and as a float
 __device__ __forceinline__ int mk_floor(float x, float &fl) {
     const float t = __fadd_rd(x, MK_MAGIC);
     fl = __fsub_rn(t, MK_MAGIC);
-    return __float_as_int(t) - MK_MAGIC_BITS;
+    return (int)(__float_as_uint(t) - (unsigned)MK_MAGIC_BITS);
 }
 __device__ __forceinline__ float mk_i2f(int i) {
     return __fsub_rn(__int_as_float(MK_MAGIC_BITS + i), MK_MAGIC);

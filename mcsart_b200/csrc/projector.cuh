@@ -374,10 +374,14 @@ struct SlabZ {
 
 // Axial part of slab d for this ray; true (and w filled) if the footprint is
 // a 2x2 window whose weights the branch-free division computed exactly.
-// zsafe: the ray's axial coordinates stay below 2^22 in magnitude, where the
-// magic-number floor is exact (otherwise the caller takes the general path).
-// Voxel indices are 32-bit: volumes are validated to hold fewer than 2^31
-// voxels (the reference indexes with int as well).
+// zsafe: the ray's axial coordinates stay inside the range of the
+// magic-number floor (otherwise the caller takes the general path).  CHECK:
+// test the division's operand range here; without it the caller has shown it
+// for every slab of the ray (ray_axial).  The four candidates' addresses are
+// clamped to the volume, so that they can be loaded before the predicates
+// are known.  Voxel indices are 32-bit: volumes are validated to hold fewer
+// than 2^31 voxels (the reference indexes with int as well).
+template <bool CHECK>
 __device__ __forceinline__ bool slab_window(const RayGeom &r, const Geom &g, const SlabC &c, int sz,
                                             float z_half, bool zsafe, SlabZ &w) {
     // :71-77 / :124-130 ("ratio * xc + z1 + nz / 2", z1 = 0)
@@ -388,9 +392,12 @@ __device__ __forceinline__ bool slab_window(const RayGeom &r, const Geom &g, con
     const int Z1 = mk_floor(zi1, fz0), Z2 = mk_floor_i(zi2);
     const float fz1 = __fadd_rn(fz0, 1.0f);
     const float dz = __fsub_rn(zi2, zi1);
+    const unsigned nz = (unsigned)g.nz, dZ = (unsigned)Z2 - (unsigned)Z1;
+    // the reference's axial loop visits Z1 and (when Z2 = Z1 + 1) Z1 + 1,
+    // clamped to the volume (:80-82 / :133-135)
     const bool u0 = c.flags & SC_U0, u1 = c.flags & SC_U1;
-    const bool z0 = Z1 >= 0 && Z1 <= g.nz - 1;
-    const bool z1 = Z1 + 1 <= Z2 && Z1 + 1 >= 0 && Z1 + 1 <= g.nz - 1;
+    const bool z0 = (unsigned)Z1 < nz;
+    const bool z1 = dZ != 0u && (unsigned)Z1 + 1u < nz;
     w.p00 = u0 && z0;
     w.p01 = u0 && z1;
     w.p10 = u1 && z0;
@@ -402,33 +409,63 @@ __device__ __forceinline__ bool slab_window(const RayGeom &r, const Geom &g, con
     const float y = mk_recip(dz);
     w.wz0 = mk_div(n0, dz, y);
     w.wz1 = mk_div(n1, dz, y);
-    const bool exact = mk_den_ok(dz) && mk_num_ok(n0) && mk_num_ok(n1);
+    const bool exact = CHECK ? (mk_den_ok(dz) && mk_num_ok(n0) && mk_num_ok(n1)) : true;
     const int cz0i = min(max(Z1, 0), g.nz - 1), cz1i = min(max(Z1 + 1, 0), g.nz - 1);
     w.a00 = c.r0 + cz0i * sz;
     w.a01 = c.r0 + cz1i * sz;
     w.a10 = c.r1 + cz0i * sz;
     w.a11 = c.r1 + cz1i * sz;
     // outside the division's checked range the caller takes the general path
-    return (c.flags & SC_NARROW) && Z2 - Z1 <= 1 && exact && zsafe;
+    return (c.flags & SC_NARROW) && dZ <= 1u && exact && zsafe;
 }
 
-// Whether every axial footprint coordinate of the ray, rz * dc + nz/2 over
-// its slabs, stays below 2^21 in magnitude (a factor 2 inside the range of
-// the magic-number floor, for rounding).
-__device__ __forceinline__ bool ray_zsafe(const RayGeom &r, float z_half) {
-    const float dmax = 1.5f * (float)r.nd + fabsf(r.src_d) + 2.0f;
-    const float zmax = fmaxf(fabsf(r.rz0), fabsf(r.rz1)) * dmax + fabsf(z_half) + 2.0f;
-    return zmax < 0.5f * MK_MAGIC_RANGE;
+// Per-ray facts about the axial footprint over all the ray's slabs, bounded
+// from the ray's constants with rounding margins: the slab distance dc runs
+// monotonically over [dc(0), dc(nd - 1)] and cz = rz * dc + nz/2 is linear in
+// it, computed with an error below 2^-23 * max|cz|.
+//  zsafe: |cz| < 2^19, inside the magic-number floor's range, so that also
+//         dz = zi2 - zi1 < 2^20;
+//  exact: additionally dc keeps one sign, dz >= 2^-19 (|rz1 - rz0| * |dc|
+//         less the rounding) and no cz comes within 2^-50 of zero.  Then
+//         every slab's division operands are in mk_div's checked range: dz is
+//         in [2^-20, 2^20); n0 is either dz or (Z1 + 1) - zi1, a positive
+//         multiple of ulp(zi1) >= 2^-73; n1, used only when Z2 = Z1 + 1, is
+//         zi2 - (Z1 + 1), zero or a positive multiple of ulp(zi2); cz is
+//         never -0, so neither is -0.  (n1 when Z2 = Z1 is never used.)
+struct RayAxial {
+    bool zsafe, exact;
+};
+__device__ __forceinline__ RayAxial ray_axial(const RayGeom &r, float z_half) {
+    const float dc_lo = __fsub_rn(__fsub_rn(0.5f, r.d_half), r.src_d) - 1.0f;
+    const float dc_hi = __fsub_rn(__fsub_rn((float)r.nd - 0.5f, r.d_half), r.src_d) + 1.0f;
+    const float dmax = fmaxf(fabsf(dc_lo), fabsf(dc_hi));
+    const float rmax = fmaxf(fabsf(r.rz0), fabsf(r.rz1));
+    const float zmax = rmax * dmax + fabsf(z_half) + 1.0f;
+    const float err = zmax * 0x1p-21f;  // >= 4 ulp of any cz, covers these bounds' rounding
+    RayAxial a;
+    a.zsafe = zmax + err < 0x1p19f;
+    const bool one_sign = dc_lo > 0.0f || dc_hi < 0.0f;
+    const float dmin = fminf(fabsf(dc_lo), fabsf(dc_hi));
+    const float drz = fabsf(r.rz1 - r.rz0);
+    const float dz_min = (drz * dmin - 2.0f * err) * (1.0f - 0x1p-20f);
+    // the range of each cz over the ray, from its ends
+    const float e0a = fmaf(r.rz0, dc_lo, z_half), e0b = fmaf(r.rz0, dc_hi, z_half);
+    const float e1a = fmaf(r.rz1, dc_lo, z_half), e1b = fmaf(r.rz1, dc_hi, z_half);
+    const float tiny = 0x1p-50f + err;
+    const bool off0 = fminf(e0a, e0b) > tiny || fmaxf(e0a, e0b) < -tiny;
+    const bool off1 = fminf(e1a, e1b) > tiny || fmaxf(e1a, e1b) < -tiny;
+    a.exact = a.zsafe && one_sign && dz_min >= 0x1p-19f && off0 && off1;
+    return a;
 }
 
 // One slab of one ray, any footprint: the 2x2 window with predication or the
 // reference's loops (:80-88 / :133-141).
-template <int K, bool ONES, typename VT>
+template <int K, bool ONES, typename VT, bool CHECK>
 __device__ __forceinline__ void fp_slab(const RayGeom &r, const Geom &g, const SlabC &e, int d,
                                         const VT *const *base, int su, int sd, int sz,
                                         float z_half, bool zsafe, float *acc, float &accw) {
     SlabZ w;
-    if (slab_window(r, g, e, sz, z_half, zsafe, w)) {
+    if (slab_window<CHECK>(r, g, e, sz, z_half, zsafe, w)) {
 #pragma unroll
         for (int k = 0; k < K; k++) {
             if (w.p00) acc[k] = __fmaf_rn(__fmul_rn(ldv(base[k], w.a00), w.wu0), w.wz0, acc[k]);
@@ -475,7 +512,7 @@ __device__ __forceinline__ void fp_slab(const RayGeom &r, const Geom &g, const S
 // The windows of slabs d0+j .. d0+j+FPC_GROUP-1 of a ray and the 4*K voxel
 // values of each (addresses are clamped, so every load is in bounds); true if
 // all of them are exact 2x2 windows.
-template <int K, typename VT>
+template <int K, bool CHECK, typename VT>
 __device__ __forceinline__ bool fp_group_load(const RayGeom &r, const Geom &g,
                                               const SlabC (*sm_c)[FPC_COLS], int col, int j, int sz,
                                               const VT *const *base, float z_half, bool zsafe,
@@ -484,7 +521,7 @@ __device__ __forceinline__ bool fp_group_load(const RayGeom &r, const Geom &g,
     bool all_fast = true;
 #pragma unroll
     for (int q = 0; q < FPC_GROUP; q++)
-        all_fast &= slab_window(r, g, sm_c[j + q][col], sz, z_half, zsafe, w[q]);
+        all_fast &= slab_window<CHECK>(r, g, sm_c[j + q][col], sz, z_half, zsafe, w[q]);
 #pragma unroll
     for (int q = 0; q < FPC_GROUP; q++)
 #pragma unroll
@@ -499,7 +536,7 @@ __device__ __forceinline__ bool fp_group_load(const RayGeom &r, const Geom &g,
 
 // The terms of one group in the reference's order: from the loaded windows
 // when all are 2x2 (fast), else slab by slab on the general path.
-template <int K, bool ONES, typename VT>
+template <int K, bool ONES, typename VT, bool CHECK>
 __device__ __forceinline__ void fp_group_sum(const RayGeom &r, const Geom &g,
                                              const SlabC (*sm_c)[FPC_COLS], int col, int j, int d0,
                                              const VT *const *base, int su, int sd, int sz,
@@ -508,8 +545,8 @@ __device__ __forceinline__ void fp_group_sum(const RayGeom &r, const Geom &g,
     if (!fast) {
 #pragma unroll 1
         for (int q = 0; q < FPC_GROUP; q++)
-            fp_slab<K, ONES, VT>(r, g, sm_c[j + q][col], d0 + j + q, base, su, sd, sz, z_half, zsafe,
-                                 acc, accw);
+            fp_slab<K, ONES, VT, CHECK>(r, g, sm_c[j + q][col], d0 + j + q, base, su, sd, sz, z_half,
+                                        zsafe, acc, accw);
         return;
     }
 #pragma unroll
@@ -551,6 +588,30 @@ __device__ __forceinline__ void fp_group_sum(const RayGeom &r, const Geom &g,
             if (x.p11) accw = __fmaf_rn(x.wu1, x.wz1, accw);
         }
     }
+}
+
+// Slabs d0 .. d0 + dn - 1 of a ray from the shared table.  Groups of
+// FPC_GROUP slabs: the windows and loads of a whole group are issued together
+// before its terms enter the sums in the reference's order, so that a warp
+// waits for memory once per group instead of per slab.  A group whose
+// footprints are not all 2x2 windows takes the general per-slab path.
+template <int K, bool ONES, typename VT, bool CHECK>
+__device__ __forceinline__ void fp_chunk(const RayGeom &r, const Geom &g,
+                                         const SlabC (*sm_c)[FPC_COLS], int col, int dn, int d0,
+                                         const VT *const *base, int su, int sd, int sz, float z_half,
+                                         bool zsafe, float *acc, float &accw) {
+    const int ng = dn / FPC_GROUP;
+    for (int i = 0; i < ng; i++) {
+        SlabZ w[FPC_GROUP];
+        float v[FPC_GROUP][K][4];
+        const bool fast = fp_group_load<K, CHECK>(r, g, sm_c, col, i * FPC_GROUP, sz, base, z_half,
+                                                  zsafe, w, v);
+        fp_group_sum<K, ONES, VT, CHECK>(r, g, sm_c, col, i * FPC_GROUP, d0, base, su, sd, sz,
+                                         z_half, zsafe, fast, w, v, acc, accw);
+    }
+    for (int j = ng * FPC_GROUP; j < dn; j++)
+        fp_slab<K, ONES, VT, CHECK>(r, g, sm_c[j][col], d0 + j, base, su, sd, sz, z_half, zsafe, acc,
+                                    accw);
 }
 
 // blockDim = FPC_THREADS: thread t is column t % FPC_COLS, row t / FPC_COLS;
@@ -602,7 +663,10 @@ __global__ void __launch_bounds__(FPC_THREADS, K == 1 ? FPC_MIN_BLOCKS_K1 : FPC_
 #pragma unroll
     for (int k = 0; k < K; k++) acc[k] = 0.0f;
 
-    const bool zsafe = ray_zsafe(r, z_half);
+    // warps whose rays all have proven division operands skip the per-slab
+    // range checks (warp-uniform, so neither form diverges)
+    const RayAxial ax = ray_axial(r, z_half);
+    const bool warp_exact = __all_sync(0xffffffffu, !active || ax.exact);
     const int nd_max = max(g.nx, g.ny);
     for (int d0 = 0; d0 < nd_max; d0 += FPC_CHUNK) {
         for (int j = row; j < FPC_CHUNK; j += FPC_ROWS) {
@@ -615,23 +679,12 @@ __global__ void __launch_bounds__(FPC_THREADS, K == 1 ? FPC_MIN_BLOCKS_K1 : FPC_
         }
         __syncthreads();
         const int dn = active ? min(FPC_CHUNK, r.nd - d0) : 0;
-        // Groups of FPC_GROUP slabs: the windows and the (always in-bounds)
-        // loads of a whole group are issued together before its terms enter
-        // the sums in the reference's order, so that a warp waits for memory
-        // once per group instead of per slab.  A group whose footprints are
-        // not all 2x2 windows takes the general per-slab path.
-        const int ng = dn / FPC_GROUP;
-        for (int i = 0; i < ng; i++) {
-            SlabZ w[FPC_GROUP];
-            float v[FPC_GROUP][K][4];
-            const bool fast = fp_group_load<K>(r, g, sm_c, col, i * FPC_GROUP, sz, base, z_half,
-                                               zsafe, w, v);
-            fp_group_sum<K, ONES, VT>(r, g, sm_c, col, i * FPC_GROUP, d0, base, su, sd, sz, z_half,
-                                      zsafe, fast, w, v, acc, accw);
-        }
-        for (int j = ng * FPC_GROUP; j < dn; j++)
-            fp_slab<K, ONES, VT>(r, g, sm_c[j][col], d0 + j, base, su, sd, sz, z_half, zsafe, acc,
-                                 accw);
+        if (warp_exact)
+            fp_chunk<K, ONES, VT, false>(r, g, sm_c, col, dn, d0, base, su, sd, sz, z_half, ax.zsafe,
+                                         acc, accw);
+        else
+            fp_chunk<K, ONES, VT, true>(r, g, sm_c, col, dn, d0, base, su, sd, sz, z_half, ax.zsafe,
+                                        acc, accw);
         __syncthreads();
     }
 
