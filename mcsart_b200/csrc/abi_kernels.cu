@@ -135,7 +135,10 @@ MC_EXPORT int mcsart_backprojection(mcsart_ctx *ctx, float *d_img, const float *
     a.angle = angle;
     a.out = d_img;
     const dim3 grid(div_up(nx, 32), div_up(ny, BP_ROWS), div_up(nz, BP_NZ)), block(32, BP_ROWS);
-    MC_LAUNCH(ctx, (bp_kernel<1, BP_PLAIN>), grid, block, 0, a);
+    if (bp_geom_proven(g))
+        MC_LAUNCH(ctx, (bp_kernel<1, BP_PLAIN, false, true>), grid, block, 0, a);
+    else
+        MC_LAUNCH(ctx, (bp_kernel<1, BP_PLAIN>), grid, block, 0, a);
     return finish(ctx, "mcsart_backprojection");
 }
 

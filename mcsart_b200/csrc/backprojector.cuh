@@ -31,6 +31,9 @@ struct BPColumn {
     float rl, rr, r0;  // magnifications SD/(x+SO) at the three distances
 };
 
+// PROVEN: bp_geom_proven(g) holds, so every division below has its operands
+// in mk_div's checked range and takes the branch-free form without tests.
+template <bool PROVEN>
 __device__ __forceinline__ BPColumn bp_column(int ix, int iy, float cphi, float sphi,
                                               const Geom &g) {
     const float xc = (float)ix - g.nx / 2 + 0.5f;
@@ -43,15 +46,22 @@ __device__ __forceinline__ BPColumn bp_column(int ix, int iy, float cphi, float 
     const float u = __fmaf_rn(yc, cphi, __fmul_rn(-xc, sphi));
     const float tl = t - 0.5f, tr = t + 0.5f, ul = u - 0.5f, ur = u + 0.5f;
     BPColumn c;
-    c.rl = g.SD / (tl + g.SO);  // points ll and lr
-    c.rr = g.SD / (tr + g.SO);  // points rr and rl
-    c.r0 = g.SD / (t + g.SO);   // top and bottom
+    if (PROVEN) {
+        const float dl = tl + g.SO, dr = tr + g.SO, d0 = t + g.SO;
+        c.rl = mk_div(g.SD, dl, mk_recip(dl));
+        c.rr = mk_div(g.SD, dr, mk_recip(dr));
+        c.r0 = mk_div(g.SD, d0, mk_recip(d0));
+    } else {
+        c.rl = g.SD / (tl + g.SO);  // points ll and lr
+        c.rr = g.SD / (tr + g.SO);  // points rr and rl
+        c.r0 = g.SD / (t + g.SO);   // top and bottom
+    }
     const float all = c.rl * ul, alr = c.rl * ur, arr = c.rr * ur, arl = c.rr * ul, at = c.r0 * u;
     const float amax = fmaxf(fmaxf(fmaxf(all, arr), fmaxf(alr, arl)), at);
     const float amin = fminf(fminf(fminf(all, arr), fminf(alr, arl)), at);
     const float ya = mk_recip(g.da);
     float qmax = mk_div(amax, g.da, ya), qmin = mk_div(amin, g.da, ya);
-    if (!(mk_den_ok(g.da) && mk_num_ok(amax) && mk_num_ok(amin))) {
+    if (!PROVEN && !(mk_den_ok(g.da) && mk_num_ok(amax) && mk_num_ok(amin))) {
         qmax = amax / g.da;
         qmin = amin / g.da;
     }
@@ -61,6 +71,7 @@ __device__ __forceinline__ BPColumn bp_column(int ix, int iy, float cphi, float 
 }
 
 // Axial part for slice iz (:68,96-97,115-122,137-138): detector row box.
+template <bool PROVEN>
 __device__ __forceinline__ void bp_rows(const BPColumn &c, int iz, const Geom &g, float &bmin,
                                         float &bmax) {
     const float zc = (float)iz - g.nz / 2 + 0.5f;
@@ -69,12 +80,37 @@ __device__ __forceinline__ void bp_rows(const BPColumn &c, int iz, const Geom &g
     const float lo = fminf(fminf(fminf(bl, br), fminf(bl, br)), fminf(bt, bb));
     const float y = mk_recip(g.db);
     float qhi = mk_div(hi, g.db, y), qlo = mk_div(lo, g.db, y);
-    if (!(mk_den_ok(g.db) && mk_num_ok(hi) && mk_num_ok(lo))) {
+    if (!PROVEN && !(mk_den_ok(g.db) && mk_num_ok(hi) && mk_num_ok(lo))) {
         qhi = hi / g.db;
         qlo = lo / g.db;
     }
     bmax = qhi - g.bi + 0.5f;
     bmin = qlo - g.bi + 0.5f;
+}
+
+// Whether the geometry alone puts every division of bp_column / bp_rows in
+// mk_div's checked range (divisor in [2^-20, 2^20), numerator +0 or in
+// [2^-80, 2^80]), for every voxel and angle:
+//  * |t| <= nx/2 + ny/2 + 2 for a voxel centre (|sin|, |cos| <= 1), so the
+//    magnification divisors t -+ 0.5 + SO lie in [SO - R, SO + R] and the
+//    magnifications r = SD / divisor in [rmin, rmax];
+//  * the column box ends are corner products r * (u -+ 0.5) (the centre
+//    product r0 * u lies between them): u -+ 0.5 is +0 or at least 2^-25 in
+//    magnitude (an exact difference of floats near 0.5 when it is small);
+//  * the row box ends are r times a half-integer, or r0 times an integer,
+//    which is +0 or at least 1 in magnitude.
+// None of these is -0.  Bounds carry a margin of 2^-10 for rounding and for
+// the intrinsic sine and cosine.
+inline bool bp_geom_proven(const Geom &g) {
+    const double R = ((double)(g.nx / 2) + (double)(g.ny / 2) + 3.0) * (1.0 + 0x1p-10);
+    const double dlo = (double)g.SO - R, dhi = (double)g.SO + R;
+    if (!(dlo >= 0x1p-19 && dhi < 0x1p19)) return false;
+    const double rmin = (double)g.SD / dhi * (1.0 - 0x1p-10);
+    const double rmax = (double)g.SD / dlo * (1.0 + 0x1p-10);
+    const double extent = R + (double)(g.nz / 2) + 4.0;
+    return g.SD >= 0x1p-79 && g.SD <= 0x1p79 && g.da >= 0x1p-19 && g.da < 0x1p19 &&
+           g.db >= 0x1p-19 && g.db < 0x1p19 && rmin * 0x1p-26 >= 0x1p-79 &&
+           rmax * extent <= 0x1p79;
 }
 
 struct BPArgs {
@@ -116,14 +152,14 @@ constexpr int BP_WB = 4;
 // reference's order (detector column outer, row inner, acc = fma(wa*wb, p,
 // acc), :150-168).  The column box and the column weights wa are shared by the
 // voxels of a thread, the row weights wb are computed once per voxel.
-template <int K>
+template <int K, bool PROVEN>
 __device__ __forceinline__ void bp_gather_view(const BPArgs &p, float angle, const float *proj,
                                                const float2 *pair, int ix, int iy, int z0,
                                                float *acc0, float *acc1) {
     const Geom &g = p.g;
     const int na = g.na;
     const float sphi = __sinf(angle), cphi = __cosf(angle);
-    const BPColumn col = bp_column(ix, iy, cphi, sphi, g);
+    const BPColumn col = bp_column<PROVEN>(ix, iy, cphi, sphi, g);
     // rows of each slice: first row, count (BP_WB + 1 = more than BP_WB),
     // row weights, box
     int ib0[BP_NZ], nbk[BP_NZ];
@@ -138,7 +174,7 @@ __device__ __forceinline__ void bp_gather_view(const BPArgs &p, float angle, con
         for (int j = 0; j < BP_WB; j++) wb[k][j] = 0.0f;
         const int iz = z0 + k;
         if (iz < g.nz) {
-            bp_rows(col, iz, g, bmn[k], bmx[k]);
+            bp_rows<PROVEN>(col, iz, g, bmn[k], bmx[k]);
             const float blim = ((float)g.nb < bmx[k]) ? (float)g.nb : bmx[k];  // MIN(nb, b_max)
             ib0[k] = max(0, (int)floorf(fmaxf(bmn[k], -1.0f)));
             // rows ib >= ib0 with (float)ib < blim, i.e. ib < ceil(blim)
@@ -198,7 +234,7 @@ __device__ __forceinline__ void bp_gather_view(const BPArgs &p, float angle, con
 // MULTI = false: one view (the reference's loop); the view loop and the
 // per-view outputs exist only in the ordered-subset instantiation, so that
 // the single-view kernel keeps its registers (and resident blocks).
-template <int K, int MODE, bool MULTI = false>
+template <int K, int MODE, bool MULTI = false, bool PROVEN = false>
 __global__ void __launch_bounds__(256, MCSART_BP_MINBLOCKS) bp_kernel(const BPArgs p) {
     __shared__ float tile[BP_NZ][BP_ROWS][33];
     const Geom &g = p.g;
@@ -217,7 +253,7 @@ __global__ void __launch_bounds__(256, MCSART_BP_MINBLOCKS) bp_kernel(const BPAr
 #pragma unroll
         for (int k = 0; k < BP_NZ; k++) { acc0[k] = 0.0f; acc1[k] = 0.0f; }
         const float angle = MULTI ? p.angles[v] : p.angle;
-        if (active) bp_gather_view<K>(p, angle, p.proj, p.pair + v * NP, ix, iy, z0, acc0, acc1);
+        if (active) bp_gather_view<K, PROVEN>(p, angle, p.proj, p.pair + v * NP, ix, iy, z0, acc0, acc1);
 #pragma unroll
         for (int k = 0; k < BP_NZ; k++) {
             const int iz = z0 + k;

@@ -186,11 +186,16 @@ template <typename ST, int INTERP, int SUM> struct Runner {
         b.outT = outT;
         const dim3 grid(div_up(P.g.nx, 32), div_up(P.g.ny, BP_ROWS), div_up(P.g.nz, BP_NZ)),
             block(32, BP_ROWS);
-        if (mode == BP_DIV) {
-            ctx->label = "bp_div";
+        // the proven form skips the division range checks (bp_geom_proven)
+        const bool proven = bp_geom_proven(P.g);
+        ctx->label = mode == BP_DIV ? "bp_div" : "bp_div_add";
+        if (mode == BP_DIV && proven) {
+            MC_LAUNCH(ctx, (bp_kernel<2, BP_DIV, false, true>), grid, block, 0, b);
+        } else if (mode == BP_DIV) {
             MC_LAUNCH(ctx, (bp_kernel<2, BP_DIV>), grid, block, 0, b);
+        } else if (proven) {
+            MC_LAUNCH(ctx, (bp_kernel<2, BP_DIV_ADD, false, true>), grid, block, 0, b);
         } else {
-            ctx->label = "bp_div_add";
             MC_LAUNCH(ctx, (bp_kernel<2, BP_DIV_ADD>), grid, block, 0, b);
         }
         return MCSART_OK;
@@ -236,11 +241,15 @@ template <typename ST, int INTERP, int SUM> struct Runner {
         for (int j = 0; j < kk && surfs; j++) b.outSurfs[j] = surfs[j];
         const dim3 grid(div_up(P.g.nx, 32), div_up(P.g.ny, BP_ROWS), div_up(P.g.nz, BP_NZ)),
             block(32, BP_ROWS);
-        if (mode == BP_DIV) {
-            ctx->label = "bp_div";
+        const bool proven = bp_geom_proven(P.g);
+        ctx->label = mode == BP_DIV ? "bp_div" : "bp_div_add";
+        if (mode == BP_DIV && proven) {
+            MC_LAUNCH(ctx, (bp_kernel<2, BP_DIV, true, true>), grid, block, 0, b);
+        } else if (mode == BP_DIV) {
             MC_LAUNCH(ctx, (bp_kernel<2, BP_DIV, true>), grid, block, 0, b);
+        } else if (proven) {
+            MC_LAUNCH(ctx, (bp_kernel<2, BP_DIV_ADD, true, true>), grid, block, 0, b);
         } else {
-            ctx->label = "bp_div_add";
             MC_LAUNCH(ctx, (bp_kernel<2, BP_DIV_ADD, true>), grid, block, 0, b);
         }
         return MCSART_OK;
