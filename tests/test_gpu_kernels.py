@@ -71,6 +71,41 @@ def test_backprojection_matches_reference_and_oracle(ctx, torch_cuda, ref, oracl
         assert rel_l2(mine, o) <= 1e-4, (a, rel_l2(mine, o))
 
 
+def bp_geom_proven(g):
+    """The condition under which the backprojector launches its form without
+    division range tests (bp_geom_proven in csrc/backprojector.cuh)."""
+    R = ((g["nx"] // 2) + (g["ny"] // 2) + 3.0) * (1.0 + 2.0 ** -10)
+    dlo, dhi = g["SO"] - R, g["SO"] + R
+    if not (dlo >= 2.0 ** -19 and dhi < 2.0 ** 19):
+        return False
+    rmin = g["SD"] / dhi * (1.0 - 2.0 ** -10)
+    rmax = g["SD"] / dlo * (1.0 + 2.0 ** -10)
+    ext = R + g["nz"] // 2 + 4.0
+    return (2.0 ** -79 <= g["SD"] <= 2.0 ** 79 and 2.0 ** -19 <= g["da"] < 2.0 ** 19
+            and 2.0 ** -19 <= g["db"] < 2.0 ** 19 and rmin * 2.0 ** -26 >= 2.0 ** -79
+            and rmax * ext <= 2.0 ** 79)
+
+
+# source 20 voxels from the centre of a 24x20 slice (half-diagonal 15.6): the
+# geometry is fine, but outside the backprojector's proof
+CLOSE = geo(nx=24, ny=20, nz=16, na=40, nb=28, SO=20, SD=30, da=0.9, db=0.8)
+
+
+def test_backprojection_outside_the_geometry_proof_matches_reference(ctx, torch_cuda, ref):
+    """Both backprojector forms are covered: the parity geometries above take
+    the one without range tests, this close-source geometry the general one;
+    each matches the reference bit for bit (and so does the projector)."""
+    assert all(bp_geom_proven(g) for g in GEOS) and not bp_geom_proven(CLOSE)
+    rng = np.random.default_rng(31)
+    img = volume((CLOSE["nz"], CLOSE["ny"], CLOSE["nx"]), seed=32)
+    for a in ANGLES:
+        proj = rng.random((CLOSE["nb"], CLOSE["na"]), dtype=np.float32)
+        np.testing.assert_array_equal(_bp(ctx, torch_cuda, proj, a, CLOSE),
+                                      ref.backprojection(proj, a, CLOSE))
+        np.testing.assert_array_equal(_fp(ctx, torch_cuda, img, a, CLOSE),
+                                      ref.projection(img, a, CLOSE))
+
+
 @pytest.mark.parametrize("shape", [(12, 20, 20), (16, 20, 24), (9, 17, 33)])
 @pytest.mark.parametrize("vf", [(0.0, 0.0), (1.3, -0.4), (-2.7, 0.9)])
 def test_deform_matches_reference(ctx, torch_cuda, ref, oracle, shape, vf):
