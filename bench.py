@@ -212,6 +212,18 @@ def cpu_threads() -> int:
         return os.cpu_count() or 1
 
 
+def cpu_model() -> str:
+    """The host CPU's model name, recorded beside the CPU baseline."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def reference_gpu_step(p) -> dict:
     """The reference's own CUDA code (host_AUMISART rebuilt from its unmodified
     sources into oracle/_ref) timed on this GPU for one step of the same
@@ -279,7 +291,8 @@ def run_reference_arm(args, rank: int):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": config_dict(p, args),
             "cpu_baseline": {"value": value, "unit": "iterations/s", "cores": threads,
-                             "kind": "port", "sample": sample},
+                             "kind": "port", "sample": sample, "cpu_model": cpu_model(),
+                             "host_cpus": os.cpu_count()},
             "e2e": {"value": value, "unit": "iterations/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0},
             "note": "the reference has no CPU implementation; this is the FP32 OpenMP "
@@ -512,7 +525,8 @@ def main():
         dt, rate, views = cpu_sample(p, h_proj_np, views, threads)
         cpu = {"value": rate, "unit": "iterations/s", "cores": threads, "kind": "port",
                "sample": f"{views} views of the image pass + {views - 1} of the DVF-update "
-                         f"pass ({dt:.1f} s), extrapolated to {nv} + {nv - 1} views"}
+                         f"pass ({dt:.1f} s), extrapolated to {nv} + {nv - 1} views",
+               "cpu_model": cpu_model(), "host_cpus": os.cpu_count()}
 
     if rank == 0:
         line = {"metric": "McSART iterations/s", "value": value, "unit": "iterations/s",
