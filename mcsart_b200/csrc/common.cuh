@@ -67,6 +67,7 @@ struct mcsart_ctx {
     std::vector<cudaEvent_t> prof_pool;
     std::vector<std::pair<std::string, ProfAgg>> prof_table;
     int device = 0;
+    int sms = 0;  // the device's SM count
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;
     int synchronous = 0;

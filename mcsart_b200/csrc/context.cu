@@ -219,8 +219,11 @@ MC_EXPORT int mcsart_create(mcsart_ctx **out, int device) {
     }
     MC_REQUIRE(device >= 0 && device < n, "device %d out of range [0, %d)", device, n);
     MC_CHECK_CUDA(cudaSetDevice(device));
+    int sms = 0;
+    MC_CHECK_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
     auto *ctx = new mcsart_ctx();
     ctx->device = device;
+    ctx->sms = sms;
     const cudaError_t es = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking);
     if (es != cudaSuccess) {
         delete ctx;

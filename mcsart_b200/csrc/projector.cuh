@@ -511,16 +511,15 @@ __device__ __forceinline__ void fp_slab(const RayGeom &r, const Geom &g, const S
     }
 }
 
-// The windows of slabs d0+j .. d0+j+fp_group<K>()-1 of a ray and the 4*K voxel
+// The windows of slabs d0+j .. d0+j+G-1 of a ray and the 4*K voxel
 // values of each (addresses are clamped, so every load is in bounds); true if
 // all of them are exact 2x2 windows.
-template <int K, bool CHECK, typename VT>
+template <int K, int G, bool CHECK, typename VT>
 __device__ __forceinline__ bool fp_group_load(const RayGeom &r, const Geom &g,
                                               const SlabC (*sm_c)[FPC_COLS], int col, int j, int sz,
                                               const VT *const *base, float z_half, bool zsafe,
                                               SlabZ *w,
                                               float (*v)[K][4]) {
-    constexpr int G = fp_group<K>();
     bool all_fast = true;
 #pragma unroll
     for (int q = 0; q < G; q++)
@@ -539,13 +538,12 @@ __device__ __forceinline__ bool fp_group_load(const RayGeom &r, const Geom &g,
 
 // The terms of one group in the reference's order: from the loaded windows
 // when all are 2x2 (fast), else slab by slab on the general path.
-template <int K, bool ONES, typename VT, bool CHECK>
+template <int K, int G, bool ONES, typename VT, bool CHECK>
 __device__ __forceinline__ void fp_group_sum(const RayGeom &r, const Geom &g,
                                              const SlabC (*sm_c)[FPC_COLS], int col, int j, int d0,
                                              const VT *const *base, int su, int sd, int sz,
                                              float z_half, bool zsafe, bool fast, const SlabZ *w,
                                              const float (*v)[K][4], float *acc, float &accw) {
-    constexpr int G = fp_group<K>();
     if (!fast) {
 #pragma unroll 1
         for (int q = 0; q < G; q++)
@@ -594,24 +592,23 @@ __device__ __forceinline__ void fp_group_sum(const RayGeom &r, const Geom &g,
     }
 }
 
-// Slabs d0 .. d0 + dn - 1 of a ray from the shared table.  Groups of
-// fp_group<K>() slabs: the windows and loads of a whole group are issued together
+// Slabs d0 .. d0 + dn - 1 of a ray from the shared table.  Groups of G
+// slabs: the windows and loads of a whole group are issued together
 // before its terms enter the sums in the reference's order, so that a warp
 // waits for memory once per group instead of per slab.  A group whose
 // footprints are not all 2x2 windows takes the general per-slab path.
-template <int K, bool ONES, typename VT, bool CHECK>
+template <int K, int G, bool ONES, typename VT, bool CHECK>
 __device__ __forceinline__ void fp_chunk(const RayGeom &r, const Geom &g,
                                          const SlabC (*sm_c)[FPC_COLS], int col, int dn, int d0,
                                          const VT *const *base, int su, int sd, int sz, float z_half,
                                          bool zsafe, float *acc, float &accw) {
-    constexpr int G = fp_group<K>();
     const int ng = dn / G;
     for (int i = 0; i < ng; i++) {
         SlabZ w[G];
         float v[G][K][4];
-        const bool fast = fp_group_load<K, CHECK>(r, g, sm_c, col, i * G, sz, base, z_half,
+        const bool fast = fp_group_load<K, G, CHECK>(r, g, sm_c, col, i * G, sz, base, z_half,
                                                   zsafe, w, v);
-        fp_group_sum<K, ONES, VT, CHECK>(r, g, sm_c, col, i * G, d0, base, su, sd, sz,
+        fp_group_sum<K, G, ONES, VT, CHECK>(r, g, sm_c, col, i * G, d0, base, su, sd, sz,
                                          z_half, zsafe, fast, w, v, acc, accw);
     }
     for (int j = ng * G; j < dn; j++)
@@ -624,14 +621,28 @@ __device__ __forceinline__ void fp_chunk(const RayGeom &r, const Geom &g,
 // MULTI = true: several views per launch (ordered subsets, kernel-level
 // multi-view projection), view = blockIdx.z with the per-view offsets of
 // FPArgs; false: one view per launch without them.
+// Whether a launch of bx x by projector blocks is resident at once with
+// FPC_MIN_BLOCKS blocks per SM (so that the larger register budget of deeper
+// slab groups costs no occupancy).
+inline bool fp_one_wave(const mcsart_ctx *ctx, unsigned bx, unsigned by) {
+    return ctx->sms > 0 && (int64_t)bx * by <= (int64_t)FPC_MIN_BLOCKS * ctx->sms;
+}
+
 // Resident blocks per SM the register budget must allow: one volume, 6 (at
 // most 80 registers, which the kernel fits without spilling); three volumes,
 // FPC_MIN_BLOCKS.  Large detectors fill every SM, and there the one-volume
 // projector runs 6 blocks per SM instead of 5 (4.6 % less projector time at
 // 512x384 rays per view; unchanged at 256x192, where fewer blocks exist).
+// G = 4 slab groups keep more loads in flight and need the 128-register
+// budget; the one-volume projector takes them when every block of the launch
+// is resident at once (fp_one_wave), where the register budget costs no
+// occupancy.
 constexpr int FPC_MIN_BLOCKS_K1 = 6;
-template <int K, bool ONES, typename VT, typename MT = VT, bool MULTI = false>
-__global__ void __launch_bounds__(FPC_THREADS, K == 1 ? FPC_MIN_BLOCKS_K1 : FPC_MIN_BLOCKS) fp_ref_kernel(const FPArgs<VT, K, MT> p) {
+template <int K, bool ONES, typename VT, typename MT = VT, bool MULTI = false,
+          int G = fp_group<K>()>
+__global__ void __launch_bounds__(FPC_THREADS, (K == 1 && G == 2) ? FPC_MIN_BLOCKS_K1
+                                                                   : FPC_MIN_BLOCKS)
+    fp_ref_kernel(const FPArgs<VT, K, MT> p) {
     __shared__ SlabC sm_c[FPC_CHUNK][FPC_COLS];
     __shared__ double2 sm_norm[FPC_THREADS / 32];
     const Geom &g = p.g;
@@ -685,10 +696,10 @@ __global__ void __launch_bounds__(FPC_THREADS, K == 1 ? FPC_MIN_BLOCKS_K1 : FPC_
         __syncthreads();
         const int dn = active ? min(FPC_CHUNK, r.nd - d0) : 0;
         if (warp_exact)
-            fp_chunk<K, ONES, VT, false>(r, g, sm_c, col, dn, d0, base, su, sd, sz, z_half, ax.zsafe,
+            fp_chunk<K, G, ONES, VT, false>(r, g, sm_c, col, dn, d0, base, su, sd, sz, z_half, ax.zsafe,
                                          acc, accw);
         else
-            fp_chunk<K, ONES, VT, true>(r, g, sm_c, col, dn, d0, base, su, sd, sz, z_half, ax.zsafe,
+            fp_chunk<K, G, ONES, VT, true>(r, g, sm_c, col, dn, d0, base, su, sd, sz, z_half, ax.zsafe,
                                         acc, accw);
         __syncthreads();
     }

@@ -166,7 +166,11 @@ template <typename ST, int INTERP, int SUM> struct Runner {
         a.norm_part = S.norm_part.as<double2>() + (int64_t)k * fp_blocks;
         const dim3 grid(fp_bx, fp_by, 1);
         ctx->label = mode == FP_MOTION ? "fp_motion" : "fp_image";
-        if (SUM == SUM_REF) {
+        if (SUM == SUM_REF && K == 1 && fp_one_wave(ctx, fp_bx, fp_by)) {
+            // every block resident at once: deeper slab groups (fp_ref_kernel)
+            MC_LAUNCH(ctx, (fp_ref_kernel<K, ONES, VT, ST, false, 4>), grid, dim3(FPC_THREADS), 0,
+                      a);
+        } else if (SUM == SUM_REF) {
             MC_LAUNCH(ctx, (fp_ref_kernel<K, ONES, VT, ST>), grid, dim3(FPC_THREADS), 0, a);
         } else {
             const size_t smem = (size_t)groups * (K + 1) * 32 * sizeof(float);
@@ -696,6 +700,7 @@ MC_EXPORT int mcsart_batch_run(mcsart_ctx *ctx, const mcsart_problem *problems,
     while ((int)ctx->lanes.size() < n_problems) {
         std::unique_ptr<mcsart_ctx> lane(new mcsart_ctx());
         lane->device = ctx->device;
+        lane->sms = ctx->sms;
         MC_CHECK_CUDA(cudaStreamCreateWithFlags(&lane->own_stream, cudaStreamNonBlocking));
         lane->stream = lane->own_stream;
         cudaEvent_t done;
