@@ -260,6 +260,10 @@ template <typename ST, int INTERP, int SUM> struct Runner {
     }
 
     dim3 tile_grid() const { return dim3(div_up(P.g.nx, 32), div_up(P.g.ny, 32), P.g.nz); }
+    // warp_fwd_kernel / warp_back_add_kernel: 32 x (8 * WARP_ROWS) tiles
+    dim3 warp_grid() const {
+        return dim3(div_up(P.g.nx, 32), div_up(P.g.ny, 8 * WARP_ROWS), P.g.nz);
+    }
 
     int finalize_norms(const int *views_dev, int n) {
         if (n == 0) return MCSART_OK;
@@ -327,10 +331,10 @@ template <typename ST, int INTERP, int SUM> struct Runner {
         const float iflow = P.flows[0] - P.flows[v];
         ctx->label = "warp_back_add";
         if (hw) {
-            MC_LAUNCH(ctx, (warp_back_add_kernel<SrcTex, ST>), tile_grid(), dim3(32, 8), 0, P.img,
+            MC_LAUNCH(ctx, (warp_back_add_kernel<SrcTex, ST>), warp_grid(), dim3(32, 8), 0, P.img,
                       S.tv_img.surf, SrcTex{tex}, f, g.nx, g.ny, g.nz, ivolume, iflow, lam);
         } else {
-            MC_LAUNCH(ctx, (warp_back_add_kernel<SrcLinear<float>, ST>), tile_grid(), dim3(32, 8),
+            MC_LAUNCH(ctx, (warp_back_add_kernel<SrcLinear<float>, ST>), warp_grid(), dim3(32, 8),
                       0, P.img, (cudaSurfaceObject_t)0, SrcLinear<float>{lin}, f, g.nx, g.ny,
                       g.nz, ivolume, iflow, lam);
         }
@@ -353,10 +357,10 @@ template <typename ST, int INTERP, int SUM> struct Runner {
             ST *d = S.img1.as<ST>() + j * V, *dT = S.img1T.as<ST>() + j * V;
             ctx->label = "warp_fwd";
             if (hw) {
-                MC_LAUNCH(ctx, (warp_fwd_kernel<SrcTex, ST, ST>), tile_grid(), dim3(32, 8), 0, d,
+                MC_LAUNCH(ctx, (warp_fwd_kernel<SrcTex, ST, ST>), warp_grid(), dim3(32, 8), 0, d,
                           dT, SrcTex{S.tv_img.tex}, f, g.nx, g.ny, g.nz, volume, flow);
             } else {
-                MC_LAUNCH(ctx, (warp_fwd_kernel<SrcLinear<float>, ST, ST>), tile_grid(),
+                MC_LAUNCH(ctx, (warp_fwd_kernel<SrcLinear<float>, ST, ST>), warp_grid(),
                           dim3(32, 8), 0, d, dT, SrcLinear<float>{P.img}, f, g.nx, g.ny, g.nz,
                           volume, flow);
             }
@@ -404,11 +408,11 @@ template <typename ST, int INTERP, int SUM> struct Runner {
             const float flow = P.flows[v] - P.flows[0];
             ctx->label = "warp_fwd";
             if (hw) {
-                MC_LAUNCH(ctx, (warp_fwd_kernel<SrcTex, ST, ST>), tile_grid(), dim3(32, 8), 0,
+                MC_LAUNCH(ctx, (warp_fwd_kernel<SrcTex, ST, ST>), warp_grid(), dim3(32, 8), 0,
                           S.img1.as<ST>(), S.img1T.as<ST>(), SrcTex{S.tv_img.tex}, f, g.nx, g.ny,
                           g.nz, volume, flow);
             } else {
-                MC_LAUNCH(ctx, (warp_fwd_kernel<SrcLinear<float>, ST, ST>), tile_grid(),
+                MC_LAUNCH(ctx, (warp_fwd_kernel<SrcLinear<float>, ST, ST>), warp_grid(),
                           dim3(32, 8), 0, S.img1.as<ST>(), S.img1T.as<ST>(),
                           SrcLinear<float>{P.img}, f, g.nx, g.ny, g.nz, volume, flow);
             }

@@ -110,21 +110,29 @@ static __global__ void __launch_bounds__(256) deform2_kernel(float *out, const f
     }
 }
 
+// Rows of voxels per thread in the image pass's warp kernels: a block covers
+// a 32 x (8 * WARP_ROWS) (x, y) tile of one slice.  2 measured best: 4 rows
+// leave a 128x128x96 volume's 1536 blocks in 1.3 waves (warp_fwd 11 % slower
+// there), 1 row costs 8 % at 256x256x160.
+constexpr int WARP_ROWS = 2;
+
 // SART image pass, forward warp of the current volume into the view's phase:
 // dst[id] = warp(src)[id] stored in VT, plus the y-fastest copy
 // dstT[iy + ix*ny] of the result (x-fastest reading) for the projector.
-// blockDim (32, 8); block covers a 32x32 (x, y) tile of slice blockIdx.z.
+// blockDim (32, 8); block covers a 32 x (8 * WARP_ROWS) (x, y) tile of slice
+// blockIdx.z.
 template <typename SRC, typename FT, typename VT>
 static __global__ void __launch_bounds__(256) warp_fwd_kernel(VT *dst, VT *dstT, const SRC src,
                                                               Fields<FT> f, int nx, int ny,
                                                               int nz, float volume, float flow) {
-    __shared__ float tile[32][33];
+    constexpr int TH = 8 * WARP_ROWS;
+    __shared__ float tile[TH][33];
     const int tx = threadIdx.x, ty = threadIdx.y;
-    const int x0 = blockIdx.x * 32, y0 = blockIdx.y * 32, iz = blockIdx.z;
+    const int x0 = blockIdx.x * 32, y0 = blockIdx.y * TH, iz = blockIdx.z;
     const int64_t slice = (int64_t)iz * nx * ny;
     const int xm = x0 + tx;
 #pragma unroll
-    for (int k = 0; k < 4; k++) {
+    for (int k = 0; k < WARP_ROWS; k++) {
         const int ly = ty + 8 * k, ym = y0 + ly;
         float v = 0.0f;
         if (xm < nx && ym < ny) {
@@ -137,11 +145,13 @@ static __global__ void __launch_bounds__(256) warp_fwd_kernel(VT *dst, VT *dstT,
         tile[ly][tx] = v;
     }
     __syncthreads();
-    const int ymT = y0 + tx;
+    // transposed store: runs of TH consecutive iy per ix
+    const int t = ty * 32 + tx;
 #pragma unroll
-    for (int k = 0; k < 4; k++) {
-        const int lx = ty + 8 * k, xmT = x0 + lx;
-        if (xmT < nx && ymT < ny) dstT[ymT + (int64_t)xmT * ny + slice] = cvt<VT>(tile[tx][lx]);
+    for (int k = 0; k < WARP_ROWS; k++) {
+        const int e = t + 256 * k, lx = e / TH, ly = e % TH;
+        const int xmT = x0 + lx, ymT = y0 + ly;
+        if (xmT < nx && ymT < ny) dstT[ymT + (int64_t)xmT * ny + slice] = cvt<VT>(tile[ly][lx]);
     }
 }
 
@@ -149,7 +159,7 @@ static __global__ void __launch_bounds__(256) warp_fwd_kernel(VT *dst, VT *dstT,
 // img[id] += lambda * warp(src)[id]  (AUMISART.cu:222-223).  With a surface,
 // the updated voxel is also written to the 3D array the next forward warp
 // samples through the texture unit.
-// blockDim (32, 8), 32x32 tiles of slice blockIdx.z (4 rows per thread).
+// blockDim (32, 8), 32 x (8 * WARP_ROWS) tiles of slice blockIdx.z.
 template <typename SRC, typename FT>
 static __global__ void __launch_bounds__(256) warp_back_add_kernel(
     float *img, cudaSurfaceObject_t img_surf, const SRC src, Fields<FT> f, int nx, int ny,
@@ -159,8 +169,8 @@ static __global__ void __launch_bounds__(256) warp_back_add_kernel(
     const int64_t slice = (int64_t)iz * nx * ny;
     if (xm >= nx) return;
 #pragma unroll
-    for (int k = 0; k < 4; k++) {
-        const int ym = blockIdx.y * 32 + ty + 8 * k;
+    for (int k = 0; k < WARP_ROWS; k++) {
+        const int ym = blockIdx.y * (8 * WARP_ROWS) + ty + 8 * k;
         if (ym >= ny) break;
         const int64_t id = xm + (int64_t)ym * nx + slice;
         int ix, iy;
