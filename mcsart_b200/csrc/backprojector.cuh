@@ -131,6 +131,11 @@ struct BPArgs {
     int n_views;
     const float *angles;
     cudaSurfaceObject_t outSurfs[16];
+    // single view: the view's column data (bp_column for every (ix, iy),
+    // index ix + iy*nx), computed by the projector launch before this one;
+    // nullptr = compute it here
+    const float4 *colA;  // amin, amax, rl, rr
+    const float *colB;   // r0
 };
 constexpr int BP_MAX_VIEWS = 16;
 
@@ -161,8 +166,19 @@ __device__ __forceinline__ void bp_gather_view(const BPArgs &p, float angle, con
                                                float *acc0, float *acc1) {
     const Geom &g = p.g;
     const int na = g.na;
-    const float sphi = __sinf(angle), cphi = __cosf(angle);
-    const BPColumn col = bp_column<PROVEN>(ix, iy, cphi, sphi, g);
+    BPColumn col;
+    if (p.colA != nullptr) {
+        const int64_t c = ix + (int64_t)iy * g.nx;
+        const float4 a = __ldg(p.colA + c);
+        col.amin = a.x;
+        col.amax = a.y;
+        col.rl = a.z;
+        col.rr = a.w;
+        col.r0 = __ldg(p.colB + c);
+    } else {
+        const float sphi = __sinf(angle), cphi = __cosf(angle);
+        col = bp_column<PROVEN>(ix, iy, cphi, sphi, g);
+    }
     // rows of each slice: first row, count (BP_WB + 1 = more than BP_WB),
     // row weights, box
     int ib0[BP_NZ], nbk[BP_NZ];

@@ -85,6 +85,7 @@ template <typename ST, int INTERP, int SUM> struct Runner {
     int fp_bx = 0, fp_by = 0, fp_blocks = 0, groups = 1;
     int subset = 1;  // views per ordered subset in image passes
     int inv_iters = 0;  // fixed-point steps of the true DVF inverse (0: negated amplitudes)
+    int cols_view = -1;  // view whose backprojector column data the last projector wrote
     std::vector<int> views_img, views_mot;
 
     Runner(mcsart_ctx *c, const Problem &p, const mcsart_options &o)
@@ -123,6 +124,8 @@ template <typename ST, int INTERP, int SUM> struct Runner {
         MC_TRY(S.ratio.ensure(vf * subset));
         MC_TRY(S.imgT.ensure(vf));
         MC_TRY(S.pairs.ensure(NP * subset * sizeof(float2)));
+        MC_TRY(S.bpcolA.ensure((size_t)P.g.nx * P.g.ny * sizeof(float4)));
+        MC_TRY(S.bpcolB.ensure((size_t)P.g.nx * P.g.ny * sizeof(float)));
         if (INTERP == MCSART_INTERP_TEXTURE && P.motion_model) {
             MC_TRY(S.tv_img.ensure(P.g.nx, P.g.ny, P.g.nz));
             MC_TRY(S.tv_ratio.ensure(P.g.nx, P.g.ny, P.g.nz));
@@ -166,6 +169,13 @@ template <typename ST, int INTERP, int SUM> struct Runner {
         a.norm_part = S.norm_part.as<double2>() + (int64_t)k * fp_blocks;
         const dim3 grid(fp_bx, fp_by, 1);
         ctx->label = mode == FP_MOTION ? "fp_motion" : "fp_image";
+        // the reference-order projector also writes the column data of this
+        // view's backprojector, which follows it
+        cols_view = SUM == SUM_REF ? v : -1;
+        if (SUM == SUM_REF) {
+            a.bpcolA = S.bpcolA.as<float4>();
+            a.bpcolB = S.bpcolB.as<float>();
+        }
         if (SUM == SUM_REF && K == 1 && fp_one_wave(ctx, fp_bx, fp_by)) {
             // every block resident at once: deeper slab groups (fp_ref_kernel)
             MC_LAUNCH(ctx, (fp_ref_kernel<K, ONES, VT, ST, false, 4>), grid, dim3(FPC_THREADS), 0,
@@ -188,6 +198,10 @@ template <typename ST, int INTERP, int SUM> struct Runner {
         b.lambda = P.lambda;
         b.out = out;
         b.outT = outT;
+        if (cols_view == v) {
+            b.colA = S.bpcolA.as<float4>();
+            b.colB = S.bpcolB.as<float>();
+        }
         const dim3 grid(div_up(P.g.nx, 32), div_up(P.g.ny, BP_ROWS), div_up(P.g.nz, BP_NZ)),
             block(32, BP_ROWS);
         // the proven form skips the division range checks (bp_geom_proven)
@@ -511,10 +525,10 @@ template <typename ST, int INTERP, int SUM> struct Runner {
         put(&P.lambda, sizeof(float));
         const void *ptrs[4] = {P.img, P.proj, P.fields, P.resid};
         put(ptrs, sizeof(ptrs));
-        const void *bufs[14] = {S.img1.ptr, S.img1T.ptr, S.imgS.ptr, S.imgST.ptr, S.img0.ptr,
+        const void *bufs[16] = {S.img1.ptr, S.img1T.ptr, S.imgS.ptr, S.imgST.ptr, S.img0.ptr,
                                 S.img0T.ptr, S.ones.ptr, S.onesT.ptr, S.ratio.ptr, S.imgT.ptr,
                                 S.pairs.ptr, S.norm_part.ptr, (const void *)S.tv_img.arr,
-                                (const void *)S.tv_ratio.arr};
+                                (const void *)S.tv_ratio.arr, S.bpcolA.ptr, S.bpcolB.ptr};
         put(bufs, sizeof(bufs));
         put(P.angles, P.n_views * sizeof(float));
         put(P.volumes, P.n_views * sizeof(float));

@@ -33,6 +33,7 @@ struct DriverState {
     // working volumes of the passes
     DevBuf img1, img1T, imgS, imgST, img0, img0T, ones, onesT, ratio, imgT;
     DevBuf pairs, norm_part, norm_tmp, views_image, views_motion, zero_fields;
+    DevBuf bpcolA, bpcolB;  // one view's backprojector column data (projector output)
     // staging for the host-pointer entry point
     DevBuf h_img, h_proj, h_fields, h_resid, h_norm;
     // 3D arrays sampled by the texture unit (INTERP_TEXTURE): the volume and
