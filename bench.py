@@ -166,7 +166,7 @@ def algorithmic_bytes(p) -> dict:
 NCU_DRAM_BYTES_C2 = {
     "fp_motion": 15459328 + 0,
     "fp_image": 5316864 + 0,
-    "bp_div": 406528 + 0,
+    "bp_div": 734208 + 0,
     "field_update_prep": 50349824 + 5771264,
 }
 
@@ -174,7 +174,7 @@ NCU_DRAM_BYTES_C2 = {
 # Issue-slot utilisation (smsp__issue_active) of the projector and
 # backprojector from the same captures: these kernels are bound by issue and
 # latency, not by HBM.
-NCU_ISSUE_ACTIVE_C2 = {"fp_image": 0.428, "fp_motion": 0.435, "bp_div": 0.769}
+NCU_ISSUE_ACTIVE_C2 = {"fp_image": 0.428, "fp_motion": 0.435, "bp_div": 0.743}
 
 
 def measured_peaks() -> dict:
