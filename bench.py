@@ -148,8 +148,9 @@ def algorithmic_bytes(p) -> dict:
         "bp_div_add": 8 * P + 12 * V,
         # read img, 6 fields; write warped volume and its y-fastest copy
         "warp_fwd": 4 * V + 24 * V + 8 * V,
-        # read ratio, 6 fields, img; write img
-        "warp_back_add": 4 * V + 24 * V + 8 * V,
+        # read ratio, 6 fields, img; write img and (texture model, the
+        # default) its 3D-array copy
+        "warp_back_add": 4 * V + 24 * V + 8 * V + 4 * V,
         # read img, 6 fields; write img0, ones and their copies
         "motion_prep": 4 * V + 24 * V + 16 * V,
         # read ratio, img, read+write 6 fields
