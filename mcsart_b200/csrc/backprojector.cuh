@@ -7,8 +7,10 @@
 // bounding box in detector index units a/da - ai + 0.5 (:135-138); unnormalised
 // overlap weights wa*wb (:150-168); __sinf/__cosf of the angle (:62-63).
 // The projection is read straight from global memory: the reference's texture
-// fetch happens at texel centres (:167) and so returns the texel itself, which
-// removes the per-call cudaMalloc3DArray + copy (:10-37).
+// fetch happens at texel centres (:167) and so returns the texel itself, with
+// denormal texels read as signed zeros (tex_texel; the projector applies it
+// to the pairs it writes for this kernel), which removes the per-call
+// cudaMalloc3DArray + copy (:10-37).
 //
 // Restructured for the hardware: one thread per column of BP_NZ voxels (no
 // atomics, so runs are bitwise reproducible), 32-wide rows of voxels per warp
@@ -220,7 +222,7 @@ __device__ __forceinline__ void bp_gather_view(const BPArgs &p, float angle, con
                         const float w = __fmul_rn(wa, wb[k][j]);
                         const int pix = ia + (ib0[k] + j) * na;
                         if (K == 1) {
-                            acc0[k] = __fmaf_rn(w, __ldg(proj + pix), acc0[k]);
+                            acc0[k] = __fmaf_rn(w, tex_texel(__ldg(proj + pix)), acc0[k]);
                         } else {
                             const float2 v = __ldg(pair + pix);
                             acc0[k] = __fmaf_rn(w, v.x, acc0[k]);
@@ -235,7 +237,7 @@ __device__ __forceinline__ void bp_gather_view(const BPArgs &p, float angle, con
                         __fmul_rn(wa, fminf(ib + 1.0f, bmx[k]) - fmaxf(ib + 0.0f, bmn[k]));
                     const int pix = ia + ib * na;
                     if (K == 1) {
-                        acc0[k] = __fmaf_rn(w, __ldg(proj + pix), acc0[k]);
+                        acc0[k] = __fmaf_rn(w, tex_texel(__ldg(proj + pix)), acc0[k]);
                     } else {
                         const float2 v = __ldg(pair + pix);
                         acc0[k] = __fmaf_rn(w, v.x, acc0[k]);

@@ -158,6 +158,16 @@ __device__ __forceinline__ float mk_i2f(int i) {
     return __fsub_rn(__int_as_float(MK_MAGIC_BITS + i), MK_MAGIC);
 }
 
+// The value the reference's backprojector reads for a projection cell: it
+// samples a linear-filtered float texture at the texel's centre
+// (src/cu_backprojection.cu:28-33,167), which returns the texel itself except
+// that a denormal texel reads as a zero of the same sign (measured on B200
+// for every sign and magnitude class).  The engine reads projections from
+// memory and applies this where the reference's read happens.
+__device__ __forceinline__ float tex_texel(float v) {
+    return fabsf(v) < 0x1p-126f ? copysignf(0.0f, v) : v;
+}
+
 __host__ __device__ inline int64_t nvox(int nx, int ny, int nz) { return (int64_t)nx * ny * nz; }
 
 int validate_geom(const Geom &g);

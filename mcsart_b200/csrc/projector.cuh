@@ -742,7 +742,9 @@ __global__ void __launch_bounds__(FPC_THREADS, (K == 1 && G == 2) ? FPC_MIN_BLOC
                 if (K >= 3) ones = acc[K - 1];                   // FP(initial2(...)), :267-268
             }
             if (p.resid) p.resid[vpix] = res;
-            p.bp_in[vpix] = make_float2(res, ones);
+            // the backprojector's operands as the reference's texture reads
+            // them; resid and the norms keep the residual itself
+            p.bp_in[vpix] = make_float2(tex_texel(res), tex_texel(ones));
             nb2 = (double)b * (double)b;
             nr2 = (double)res * (double)res;
         }
@@ -828,7 +830,7 @@ __global__ void __launch_bounds__(256) fp_kernel(const FPArgs<VT, K, MT> p) {
                 if (K >= 3) ones = s[2];            // FP(initial2(...)), :267-268
             }
             if (p.resid) p.resid[pix] = res;
-            p.bp_in[pix] = make_float2(res, ones);
+            p.bp_in[pix] = make_float2(tex_texel(res), tex_texel(ones));
             nb2 = (double)b * (double)b;
             nr2 = (double)res * (double)res;
         }

@@ -68,6 +68,35 @@ def test_warp_matches_the_reference_at_config_3(ctx, torch_cuda, ref, c3):
     np.testing.assert_array_equal(host(out), ref.deform(img, 0.7, -0.3, F))
 
 
+def test_motion_loop_matches_the_reference_at_config_3(ctx, torch_cuda):
+    """The whole host_AUMISART loop at config 3's size (256x256x160 at 1 mm,
+    detector 512x384, 660 views, breathing motion; the benchmark's seeded
+    problem): one outer iteration, an image pass and a DVF-update pass,
+    against the reference's own loop rebuilt from its sources.  Volume,
+    alpha_x and every residual projection agree bit for bit."""
+    import bench
+    from oracle import ref_runner
+    p, proj, fields = bench.build_problem(ctx, torch_cuda, "c3")
+    g, nv = p.geo, p.cfg.n_views
+    proj_h = np.ascontiguousarray(proj.cpu().numpy())
+    F = [np.ascontiguousarray(f.cpu().numpy()) for f in fields]
+    del proj, fields
+    img0 = np.ascontiguousarray(p.img0, np.float32)
+    op = np.array([1, 0], np.int32)
+    it = dict(n_iter=2, op_iter=op, n_views=nv, **{"lambda": p.cfg.lam}, outIter=1,
+              volumes=p.volumes, flows=p.flows, angles=p.angles)
+    out = dict(img=np.zeros_like(img0), resid=np.zeros((nv, g["nb"], g["na"]), np.float32),
+               norm=np.zeros(2 * nv, np.float32), alpha_x=np.zeros_like(img0))
+    ctx.host_AUMISART(out["img"], out["resid"], out["norm"], out["alpha_x"], img0, proj_h,
+                      g["nx"], g["ny"], g["nz"], g["na"], g["nb"], 1, nv, 2, op, g["da"], g["db"],
+                      g["ai"], g["bi"], g["SO"], g["SD"], 1.0, p.cfg.lam, p.volumes, p.flows,
+                      np.zeros(nv, np.float32), p.angles, *F)
+    r = ref_runner.aumisart(img0, proj_h, g, it, F)
+    np.testing.assert_array_equal(out["img"], r["img"])
+    np.testing.assert_array_equal(out["alpha_x"], r["alpha_x"])
+    np.testing.assert_array_equal(out["resid"], r["resid"])
+
+
 def test_central_rays_count_slabs_at_config_5(ctx, torch_cuda):
     torch = torch_cuda
     g = _geo("c5")
