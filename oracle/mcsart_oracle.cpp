@@ -152,8 +152,10 @@ void projection(T *proj, const T *img, double angle, double SO, double SD, doubl
 
 // ------------------------------------------------------------ backprojector
 // src/cu_backprojection.cu:49-170 for one voxel.  The reference reads the
-// projection through a linear-filtered texture exactly at texel centres
-// (:167), which returns the texel itself; it is read directly here.
+// projection through a linear-filtered float texture exactly at texel centres
+// (:167), which returns the texel itself, except that a texel below the
+// float32 normal range reads as a zero of the same sign (the texture unit's
+// behaviour, measured on B200); that read is restated here.
 template <typename T>
 T backproject_voxel(const T *proj, int ix, int iy, int iz, T cphi, T sphi, T SO, T SD, T da,
                     int na, T ai, T db, int nb, T bi, int nx, int ny, int nz) {
@@ -192,7 +194,9 @@ T backproject_voxel(const T *proj, int ix, int iy, int iz, T cphi, T sphi, T SO,
         const T wa = tmin((T)ia + 1, a_max) - tmax((T)ia, a_min);          // :156
         for (int ib = std::max(0, b_ind_min); (T)ib < b_lim; ib++) {
             const T wb = tmin((T)ib + 1, b_max) - tmax((T)ib, b_min);      // :164
-            acc += wa * wb * proj[ia + (int64_t)ib * na];                   // :167
+            const T pv = proj[ia + (int64_t)ib * na];                       // :167
+            const T tv = std::fabs(pv) < (T)0x1p-126 ? std::copysign((T)0, pv) : pv;
+            acc += wa * wb * tv;
         }
     }
     return acc;
