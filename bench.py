@@ -1,13 +1,15 @@
 """Benchmark of the McSART engine: SART iterations/s on one or more B200s.
 
-Workload (default): the motion-compensated McSART configuration, volume
-128x128x96 at 2 mm, flat detector 256x192 at 1.2 mm, SAD/SDD 1000/1500 mm,
-360 views over 360 degrees at 15 views/s with a 5DCT breathing model.  One
-step is one outer iteration = one image-update pass over all 360 views (warp,
-project, residual, backproject, normalise, inverse warp, update) plus one
-DVF-update pass over 359 views, i.e. host_AUMISART with op_iter = [1, 0].
-Inputs are seeded synthetic data of that shape (phantom, smooth random DVF,
-projections of the warped phantom), generated outside the timed region.
+Workload (default, --config c3): the motion-compensated McSART problem of
+volume 256x256x160 at 1 mm, flat detector 512x384 at 0.776 mm, SAD/SDD
+1000/1500 mm, 660 views over 360 degrees at 15 views/s with a 5DCT breathing
+model.  One step is one outer iteration = one image-update pass over all 660
+views (warp, project, residual, backproject, normalise, inverse warp, update)
+plus one DVF-update pass over 659 views, i.e. host_AUMISART with op_iter =
+[1, 0].  --config c2 selects the 128x128x96 problem (detector 256x192 at
+1.2 mm, 360 views), c1 the static 64^3 one (60 views).  Inputs are seeded
+synthetic data of that shape (phantom, smooth random DVF, projections of the
+warped phantom), generated outside the timed region.
 
   value   iterations/s through the device-resident driver, inputs in HBM,
           L2 flushed (256 MiB write) before every timed step, device time by
@@ -18,7 +20,9 @@ projections of the warped phantom), generated outside the timed region.
           memory, the iteration, D2H of image, residuals, norms, alpha_x.
   --impl reference   the reference's path on the host cores: the FP32 OpenMP
           transcription of the reference kernels (the reference has no CPU
-          code of its own), on a bounded sample of views, extrapolated.
+          code of its own), each step a bounded sample of views, the
+          iterations/s extrapolated linearly in view count; beside it, the
+          reference's own CUDA build timed on the GPU over whole steps.
 """
 from __future__ import annotations
 
@@ -42,7 +46,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
-    ap.add_argument("--config", default="c2")
+    ap.add_argument("--config", default="c3")
     ap.add_argument("--cpu-views", type=int, default=0,
                     help="views per pass in the CPU sample (0 = auto)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -162,20 +166,24 @@ def algorithmic_bytes(p) -> dict:
 
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per launch of the
-# c2 workload's kernels, from one `ncu --set full` capture of each (cold cache,
-# FP32 storage); summaries with the commands are kept under profiles/.
-NCU_DRAM_BYTES_C2 = {
-    "fp_motion": 15459328 + 0,
-    "fp_image": 5316864 + 0,
-    "bp_div": 734208 + 0,
-    "field_update_prep": 50349824 + 5771264,
+# workloads' kernels, from one ncu capture of each (cold cache, FP32
+# storage); summaries with the commands are kept under profiles/.
+NCU_DRAM_BYTES = {
+    "c2": {"fp_motion": 15459328 + 0, "fp_image": 5316864 + 0, "bp_div": 734208 + 0,
+           "field_update_prep": 50349824 + 5771264},
+    "c3": {},
 }
-
 
 # Issue-slot utilisation (smsp__issue_active) of the projector and
 # backprojector from the same captures: these kernels are bound by issue and
 # latency, not by HBM.
-NCU_ISSUE_ACTIVE_C2 = {"fp_image": 0.428, "fp_motion": 0.435, "bp_div": 0.743}
+NCU_ISSUE_ACTIVE = {"c2": {"fp_image": 0.428, "fp_motion": 0.435, "bp_div": 0.743}, "c3": {}}
+
+# Views per pass of the CPU samples: the engine line's cpu_baseline leg
+# (about 10 s of CPU work) and each step of the reference arm (a few seconds,
+# so that --steps 20 --warmup 5 ends within a few minutes).
+CPU_VIEWS = {"c1": 60, "c2": 160, "c3": 16, "c5": 4}
+REF_ARM_VIEWS = {"c1": 30, "c2": 64, "c3": 6, "c5": 2}
 
 
 def measured_peaks() -> dict:
@@ -225,11 +233,13 @@ def cpu_model() -> str:
     return "unknown"
 
 
-def reference_gpu_step(p) -> dict:
+def reference_gpu_step(p, steps: int = 3) -> dict:
     """The reference's own CUDA code (host_AUMISART rebuilt from its unmodified
-    sources into oracle/_ref) timed on this GPU for one step of the same
-    workload: its host-pointer call, with its per-call allocations, copies and
-    device reset.  Reported beside the CPU arm, not as the arm's value."""
+    sources into oracle/_ref) timed on this GPU over `steps` whole steps of
+    the same workload (after one untimed call): its host-pointer call, with
+    its per-call allocations, copies and device reset, each call in a fresh
+    process as the reference resets the device.  Reported beside the CPU
+    arm, not as the arm's value."""
     lib = os.path.join(ROOT, "oracle", "_ref", "libmcsart_ref.so")
     if not os.path.exists(lib):
         return {"unavailable": "the rebuilt reference library is not present"}
@@ -242,20 +252,22 @@ def reference_gpu_step(p) -> dict:
     from oracle import ref_runner
     ref = ref_runner.Ref()
     g = p.geo
-    proj = np.stack([ref.projection(ref.deform(p.truth, float(p.volumes[v] - p.volumes[0]),
-                                               float(p.flows[v] - p.flows[0]), p.fields),
-                                    float(p.angles[v]), g) for v in range(p.cfg.n_views)])
-    it = {"n_iter": 2, "op_iter": np.array([1, 0], np.int32), "n_views": p.cfg.n_views,
+    # measured projections made by the reference's own warp and projector
+    proj = ref.motion_projections(p.truth, p.fields, p.volumes, p.flows, p.angles, g)
+    op = np.array([1, 0], np.int32) if p.fields is not None else np.array([1], np.int32)
+    it = {"n_iter": len(op), "op_iter": op, "n_views": p.cfg.n_views,
           "lambda": p.cfg.lam, "outIter": 1, "volumes": p.volumes, "flows": p.flows,
           "angles": p.angles}
     secs = []
-    for _ in range(3):  # the first call is a warm-up
+    for _ in range(steps + 1):  # the first call is a warm-up
         r = ref_runner.aumisart(np.zeros_like(p.truth), proj, g, it, p.fields)
         secs.append(float(r["seconds"]))
-    t = float(np.median(secs[1:]))
+    s = np.array(secs[1:])
+    t = float(np.median(s))
     return {"value": 1.0 / t, "unit": "iterations/s", "seconds_per_step": t,
+            "seconds_min": float(s.min()), "seconds_max": float(s.max()),
             "kind": "reference CUDA build, host_AUMISART with host pointers",
-            "steps_timed": len(secs) - 1}
+            "steps_timed": int(len(s))}
 
 
 def run_reference_arm(args, rank: int):
@@ -269,7 +281,7 @@ def run_reference_arm(args, rank: int):
     threads = cpu_threads()
     O.set_num_threads(threads)
     proj = np.zeros((p.cfg.n_views, p.cfg.nb, p.cfg.na), np.float32)
-    views = args.cpu_views or 64
+    views = args.cpu_views or REF_ARM_VIEWS.get(args.config, 8)
     # only the views the sample touches need measured data
     for v in range(views + 1):
         vol = O.deform(p.truth, np.float32(p.volumes[v] - p.volumes[0]),
@@ -286,9 +298,12 @@ def run_reference_arm(args, rank: int):
     sample = (f"{views} views of the image pass + {views - 1} of the DVF-update pass of "
               f"{args.config} per step, extrapolated linearly to {p.cfg.n_views} + "
               f"{p.cfg.n_views - 1} views")
+    # a step of this arm is the bounded sample: ms_per_step is its measured
+    # duration, value the iterations/s extrapolated from it
     line = {"impl": "reference", "metric": "McSART iterations/s", "value": value,
             "unit": "iterations/s", "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1000.0 / value, "higher_is_better": True,
+            "warmup": args.warmup, "ms_per_step": 1000.0 * float(np.median(times)),
+            "ms_per_iteration_extrapolated": 1000.0 / value, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": config_dict(p, args),
             "cpu_baseline": {"value": value, "unit": "iterations/s", "cores": threads,
@@ -417,8 +432,8 @@ def main():
     achieved = abytes.get(top, 0) / (top_launch_ms / 1000.0) / 1e9
     roofline = {"bound": "hbm", "kernel": top, "achieved": achieved, "peak": peaks["hbm_gbs"],
                 "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
-                "traffic": NCU_DRAM_BYTES_C2.get(top) if args.config == "c2" else None,
-                "issue_active_ncu": NCU_ISSUE_ACTIVE_C2 if args.config == "c2" else None,
+                "traffic": NCU_DRAM_BYTES.get(args.config, {}).get(top),
+                "issue_active_ncu": NCU_ISSUE_ACTIVE.get(args.config) or None,
                 "peak_source": peaks["source"], "launch_ms": top_launch_ms,
                 "algorithmic_bytes_per_launch": abytes.get(top, 0),
                 "share": {k: round(v / tot_ms, 4) for k, v in kernel_ms.items()}}
@@ -454,6 +469,8 @@ def main():
            "api": "mcsart_aumisart (host pointers, pinned)"}
 
     extras = {}
+    # side measurements: a few steps each, after two untimed ones
+    xsteps = max(1, min(args.steps, 5))
     if not args.no_extras:
         # side measurements: the split-sum (Kahan) projector in FP32, 16-bit
         # storage of fields, projections and projector inputs with the
@@ -461,6 +478,7 @@ def main():
         # subsets
         for name, kw in (("split_kahan_f32", dict(fp_sum=2)),
                          ("bf16_storage", dict(storage=m.BF16, interp=m.INTERP_EXACT)),
+                         ("bf16_storage_texture_warp", dict(storage=m.BF16)),
                          ("f16_storage", dict(storage=m.F16, interp=m.INTERP_EXACT)),
                          # ordered subsets of 8 views (a different algorithm:
                          # one projector and one backprojector launch per subset)
@@ -485,12 +503,12 @@ def main():
             torch.cuda.synchronize()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            for _ in range(args.steps):
+            for _ in range(xsteps):
                 st()
             e1.record(stream)
             torch.cuda.synchronize()
             ext = max_over_ranks(e0.elapsed_time(e1) / 1000.0)
-            extras[name] = {"value": args.steps / ext * world,
+            extras[name] = {"value": xsteps / ext * world,
                             "unit": "iterations/s"}
 
         # four independent problems of this workload (different seeds) run
@@ -508,13 +526,13 @@ def main():
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        for _ in range(args.steps):
+        for _ in range(xsteps):
             ctx.batch_run(batch, n_iter=2, op_iter=op, options=drop_in)
         e1.record(stream)
         torch.cuda.synchronize()
         ext = max_over_ranks(e0.elapsed_time(e1) / 1000.0)
         extras["batch_4_problems"] = {
-            "value": nb_ * args.steps / ext * world, "unit": "iterations/s (all problems)",
+            "value": nb_ * xsteps / ext * world, "unit": "iterations/s (all problems)",
             "note": "4 independent problems of the workload, one mcsart_batch_run per step"}
         del batch
 
@@ -522,7 +540,7 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = cpu_threads()
         h_proj_np = proj.cpu().numpy()
-        views = args.cpu_views or 160
+        views = args.cpu_views or CPU_VIEWS.get(args.config, 8)
         dt, rate, views = cpu_sample(p, h_proj_np, views, threads)
         cpu = {"value": rate, "unit": "iterations/s", "cores": threads, "kind": "port",
                "sample": f"{views} views of the image pass + {views - 1} of the DVF-update "

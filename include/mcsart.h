@@ -258,9 +258,8 @@ int mcsart_batch_run(mcsart_ctx *ctx, const mcsart_problem *problems, int n_prob
  * voxels (e.g. 256x256x64), i.e. 16 MiB of FP32 scratch per device. */
 #define MCSART_NOALLOC_MAX_VOXELS 4194304
 
-/* mcsart_projection without any allocation.  No counterpart in the reference:
- * host_projection (src/cu_projection.cu:7) is the operation, this is an
- * added way to call it.
+/* mcsart_projection without any allocation.  This entry point has no
+ * counterpart in the reference.
  *
  * Who needs it.  mcsart_projection keeps a scratch copy of the volume in its
  * context and allocates it (cudaMalloc) the first time a size is seen; the
@@ -283,7 +282,10 @@ int mcsart_batch_run(mcsart_ctx *ctx, const mcsart_problem *problems, int n_prob
  * - set-up: the first call on each device, with that device current, looks
  *   up the scratch's address (cudaGetSymbolAddress) and loads the kernels.
  *   Make that first call before any stream capture and outside time-critical
- *   code; later calls on that device do no set-up;
+ *   code; later calls on that device do no set-up.  The address belongs to
+ *   the device's current CUDA context: after a cudaDeviceReset, or from
+ *   another context of the same device, the next call repeats the set-up
+ *   (so make it, too, outside a stream capture);
  * - nothing has to start at zero: the scratch is written before it is read
  *   and every cell of d_proj is written;
  * - all calls on one device share the one scratch.  Calls in one stream are

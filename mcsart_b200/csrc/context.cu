@@ -86,6 +86,10 @@ int validate_geom(const Geom &g) {
     const int lim = 1 << 20;
     MC_REQUIRE(g.nx <= lim && g.ny <= lim && g.nz <= lim && g.na <= lim && g.nb <= lim,
                "volume and detector dimensions must be at most 2^20");
+    // kernels index slices (nz) and detector rows (nb) with a grid dimension,
+    // whose limit is 65535
+    MC_REQUIRE(g.nz <= 65535, "volume depth nz must be at most 65535 (got %d)", g.nz);
+    MC_REQUIRE(g.nb <= 65535, "detector rows nb must be at most 65535 (got %d)", g.nb);
     MC_REQUIRE(g.SO > 0.0f && g.SD > 0.0f, "SO and SD must be positive");
     MC_REQUIRE(g.da > 0.0f && g.db > 0.0f, "detector pitches da, db must be positive");
     return MCSART_OK;

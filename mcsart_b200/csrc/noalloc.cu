@@ -4,6 +4,8 @@
 // fixed file-scope device array instead of a context workspace.  It allocates
 // nothing and needs no context.  The kernels and their launch shapes are those
 // of mcsart_projection, so the results are bitwise the same.
+#include <cuda.h>  // CUcontext and CUresult, for the driver calls resolved below
+
 #include <mutex>
 
 #include "common.cuh"
@@ -25,10 +27,58 @@ namespace {
 
 constexpr int kMaxDevices = 64;
 std::mutex g_setup_mu;
-float *g_scratch[kMaxDevices];  // device address of g_noalloc_volT, per device
 
-// Set-up on first use per device, with that device current: the scratch's
-// address, and both kernels loaded so that later calls load nothing.
+// The scratch's device address belongs to one CUDA context: each context
+// that loads this library's module has its own instance of the array.  A
+// cudaDeviceReset (which the reference's MEX functions call at the end of
+// every call, and which may run in the same process) or a context created
+// with the driver API gives the device a new context, and the address
+// looked up in the old one is then invalid.  So the set-up is cached per
+// device together with the unique id of the context it was done in
+// (cuCtxGetId, never reused within a process), and redone when the calling
+// thread's current context is another one.
+struct Setup {
+    unsigned long long ctx_id = 0;  // 0: not set up
+    float *scratch = nullptr;       // device address of g_noalloc_volT in that context
+};
+Setup g_setup[kMaxDevices];
+
+using PfnCtxGetCurrent = CUresult (*)(CUcontext *);
+using PfnCtxGetId = CUresult (*)(CUcontext, unsigned long long *);
+PfnCtxGetCurrent g_ctx_get_current = nullptr;
+PfnCtxGetId g_ctx_get_id = nullptr;
+
+// Driver entry points, resolved through the runtime (no link against the
+// driver library); called with g_setup_mu held.
+int resolve_driver_calls() {
+    if (g_ctx_get_current && g_ctx_get_id) return MCSART_OK;
+    void *f0 = nullptr, *f1 = nullptr;
+    cudaDriverEntryPointQueryResult q0 = cudaDriverEntryPointSymbolNotFound, q1 = q0;
+    MC_CHECK_CUDA(cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f0, 12000,
+                                                    cudaEnableDefault, &q0));
+    MC_CHECK_CUDA(cudaGetDriverEntryPointByVersion("cuCtxGetId", &f1, 12000, cudaEnableDefault,
+                                                    &q1));
+    MC_REQUIRE(q0 == cudaDriverEntryPointSuccess && q1 == cudaDriverEntryPointSuccess && f0 && f1,
+               "mcsart_projection_noalloc: the driver lacks cuCtxGetCurrent/cuCtxGetId");
+    g_ctx_get_current = reinterpret_cast<PfnCtxGetCurrent>(f0);
+    g_ctx_get_id = reinterpret_cast<PfnCtxGetId>(f1);
+    return MCSART_OK;
+}
+
+// Id of the calling thread's current context (called with g_setup_mu held).
+int current_context_id(unsigned long long *id) {
+    CUcontext c = nullptr;
+    MC_REQUIRE(g_ctx_get_current(&c) == CUDA_SUCCESS && c != nullptr,
+               "mcsart_projection_noalloc: no current CUDA context");
+    MC_REQUIRE(g_ctx_get_id(c, id) == CUDA_SUCCESS && *id != 0,
+               "mcsart_projection_noalloc: cuCtxGetId failed");
+    return MCSART_OK;
+}
+
+// Set-up on the first call per device and context, with that device
+// current: the scratch's address (cudaGetSymbolAddress, which also makes the
+// runtime's context current), and both kernels loaded so that later calls
+// load nothing.  Later calls in the same context only compare the id.
 int scratch_of_current_device(float **out) {
     int dev = -1;
     const cudaError_t e = cudaGetDevice(&dev);
@@ -40,15 +90,26 @@ int scratch_of_current_device(float **out) {
     MC_REQUIRE(dev >= 0 && dev < kMaxDevices,
                "mcsart_projection_noalloc: device ordinal %d above %d", dev, kMaxDevices - 1);
     std::lock_guard<std::mutex> lock(g_setup_mu);
-    if (g_scratch[dev] == nullptr) {
-        void *p = nullptr;
-        MC_CHECK_CUDA(cudaGetSymbolAddress(&p, g_noalloc_volT));
-        cudaFuncAttributes fa;
-        MC_CHECK_CUDA(cudaFuncGetAttributes(&fa, transpose_kernel<float, float>));
-        MC_CHECK_CUDA(cudaFuncGetAttributes(&fa, fp_ref_kernel<1, false, float>));
-        g_scratch[dev] = static_cast<float *>(p);
+    MC_TRY(resolve_driver_calls());
+    Setup &s = g_setup[dev];
+    if (s.ctx_id != 0) {
+        unsigned long long id = 0;
+        MC_TRY(current_context_id(&id));
+        if (id == s.ctx_id) {
+            *out = s.scratch;
+            return MCSART_OK;
+        }
     }
-    *out = g_scratch[dev];
+    void *p = nullptr;
+    MC_CHECK_CUDA(cudaGetSymbolAddress(&p, g_noalloc_volT));
+    cudaFuncAttributes fa;
+    MC_CHECK_CUDA(cudaFuncGetAttributes(&fa, transpose_kernel<float, float>));
+    MC_CHECK_CUDA(cudaFuncGetAttributes(&fa, fp_ref_kernel<1, false, float>));
+    unsigned long long id = 0;
+    MC_TRY(current_context_id(&id));
+    s.ctx_id = id;
+    s.scratch = static_cast<float *>(p);
+    *out = s.scratch;
     return MCSART_OK;
 }
 

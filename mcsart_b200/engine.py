@@ -45,16 +45,40 @@ def _hptr(a: np.ndarray) -> int:
 
 def projection_noalloc(d_proj, d_img, angle, SO, SD, da, na, ai, db, nb, bi, nx, ny, nz,
                        stream=None):
-    """mcsart_projection_noalloc: host_projection's operation (include/cu_projection.h:7)
-    without a context and without allocating; scratch in a fixed device array
-    of MCSART_NOALLOC_MAX_VOXELS voxels.  stream: an int cudaStream_t, a
-    torch.cuda.Stream, or None for the legacy default stream."""
+    """mcsart_projection_noalloc: the projection of mcsart_projection without a
+    context and without allocating; scratch in a fixed device array of
+    MCSART_NOALLOC_MAX_VOXELS voxels.  stream: an int cudaStream_t, a
+    torch.cuda.Stream, or None for the legacy default stream.
+
+    Torch tensors must sit on one device and hold nx*ny*nz (d_img) and na*nb
+    (d_proj) elements; the call runs with that device current.  Raw int
+    pointers are passed through unchecked, on the current device."""
     if stream is not None and not isinstance(stream, int):
         stream = stream.cuda_stream
+    p_proj, p_img = _ptr(d_proj, "d_proj", 4), _ptr(d_img, "d_img", 4)
+    tensors = [t for t in (d_proj, d_img) if hasattr(t, "is_cuda")]
+    device = None
+    if tensors:
+        devs = {t.device for t in tensors}
+        if len(devs) != 1:
+            raise ValueError(f"d_proj and d_img must be on one device (got {sorted(map(str, devs))})")
+        device = tensors[0].device
+    if hasattr(d_img, "numel") and d_img.numel() != nx * ny * nz:
+        raise ValueError(f"d_img holds {d_img.numel()} elements, nx*ny*nz = {nx * ny * nz}")
+    if hasattr(d_proj, "numel") and d_proj.numel() != na * nb:
+        raise ValueError(f"d_proj holds {d_proj.numel()} elements, na*nb = {na * nb}")
     L = _lib.load()
-    check(L.mcsart_projection_noalloc(stream, _ptr(d_proj, "d_proj", 4), _ptr(d_img, "d_img", 4),
-                                      angle, SO, SD, da, na, ai, db, nb, bi, nx, ny, nz),
-          "mcsart_projection_noalloc")
+
+    def call():
+        check(L.mcsart_projection_noalloc(stream, p_proj, p_img, angle, SO, SD, da, na, ai, db,
+                                          nb, bi, nx, ny, nz),
+              "mcsart_projection_noalloc")
+    if device is None:
+        call()
+    else:
+        import torch
+        with torch.cuda.device(device):
+            call()
 
 
 def default_options(**kw) -> Options:

@@ -1,7 +1,7 @@
 // Test infrastructure: CPU oracle for the McSART hot path (see mcsart_oracle.h).
 //
 // One templated restatement of the reference kernels, instantiated twice:
-//   T = double -> orc_*  (FP64 oracle; the checker)
+//   T = double -> orc_*  (FP64 oracle; the accuracy reference of the tests)
 //   T = float  -> cpu_*  (FP32 OpenMP transcription; the timed CPU baseline)
 // Each function cites the reference lines it restates.  Index conventions,
 // integer divisions (nx/2 vs (float)nx/2), loop bounds and the order of the

@@ -1,7 +1,7 @@
 /* Test infrastructure: the CPU oracle for the McSART hot path.
  *
  * orc_*  : FP64 restatement of every reference kernel and of the SART loop
- *          (the checker used by tests/, smoke() and bench.py's cpu_baseline leg).
+ *          (the accuracy reference used by tests/, smoke() and bench.py's cpu_baseline leg).
  * cpu_*  : the same restatement instantiated in FP32 and parallelised with
  *          OpenMP; it is the timed CPU baseline (the reference has no CPU path).
  *

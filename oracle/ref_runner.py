@@ -218,6 +218,32 @@ class Ref:
         finally:
             self._free()
 
+    def motion_projections(self, truth, fields, volumes, flows, angles, geo):
+        """proj_v = host_projection(host_deform(truth, a_v - a_0, b_v - b_0), angle_v)
+        for every view, with the volume and fields uploaded once (the
+        measured projections of a motion workload, made by the reference's
+        own kernels); fields None: the static truth's projections."""
+        try:
+            nz, ny, nx = truth.shape
+            shape = (geo["nb"], geo["na"])
+            d_truth = self._up(truth)
+            d_tmp = self._new(truth.size * 4)
+            d_f = [self._up(f) for f in fields] if fields is not None else None
+            d_proj = self._new(int(np.prod(shape)) * 4)
+            out = np.empty((len(angles),) + shape, np.float32)
+            for v, a in enumerate(angles):
+                src = d_truth
+                if d_f is not None:
+                    self.L.ref_deform(d_tmp, d_truth, nx, ny, nz,
+                                      float(np.float32(volumes[v] - volumes[0])),
+                                      float(np.float32(flows[v] - flows[0])), *d_f)
+                    src = d_tmp
+                self.L.ref_projection(d_proj, src, float(a), *self._g(geo))
+                out[v] = self._down(d_proj, shape)
+            return out
+        finally:
+            self._free()
+
     # ------------------------------------------------------ the SART loop
     def aumisart_inprocess(self, img, proj, geo, it, fields=None):
         """host_AUMISART in this process; ends in cudaDeviceReset()."""

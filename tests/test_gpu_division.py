@@ -1,6 +1,6 @@
 """The branch-free division the projector and backprojector use instead of
 the compiler's (mk_recip / mk_div, Markstein's method) must round exactly as
-__frcp_rn / __fdiv_rn: a checker compiled from the library's own header runs
+__frcp_rn / __fdiv_rn: a test program compiled from the library's own header runs
 every divisor significand for exponents -20 .. 19 (3.4e8 reciprocals, 1.3e9
 quotients) and 2.4e9 random quotients.  The magic-number floor and
 int-to-float conversions are checked for every float below 2^22 in

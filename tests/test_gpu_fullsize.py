@@ -1,8 +1,8 @@
 """Parity at the benchmark's full sizes.
 
 The kernel-level parity tests use small volumes the CPU oracle finishes in
-seconds.  Here the projector, backprojector and warp run at SURVEY config 3's
-size (256x256x160, detector 512x384) against the reference's own kernels,
+seconds.  Here the projector, backprojector and warp run at the full size of the
+256x256x160 motion-compensated workload (detector 512x384, 660 views) against the reference's own kernels,
 rebuilt from its sources, bit for bit; and at config 5's size (512x512x256,
 detector 1024x768) a size-independent property: a ray that stays inside the
 volume through every slab sums normalised footprint weights, so its projection

@@ -1,7 +1,7 @@
 """The reference's backprojector reads each projection cell through a
 linear-filtered texture at the texel's centre; the engine reads memory and
 applies tex_texel (csrc/common.cuh): the texel itself, denormals as signed
-zeros.  A checker compiled from the library's own header compares tex_texel
+zeros.  A test program compiled from the library's own header compares tex_texel
 with the texture unit on 65536 texels of every sign and magnitude class."""
 import os
 import subprocess

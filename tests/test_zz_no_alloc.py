@@ -87,3 +87,15 @@ def test_noalloc_on_the_legacy_default_stream(torch_cuda):
         ctx.close()
     torch.cuda.synchronize()
     np.testing.assert_array_equal(out.cpu().numpy(), ref.cpu().numpy())
+
+
+def test_depth_beyond_the_grid_limit_is_rejected_before_any_device_work():
+    """A volume within the voxel limit whose depth exceeds the 65535 slices a
+    launch grid can index is refused with a message, without device work."""
+    from mcsart_b200 import _lib
+    L = _lib.load()
+    g = geo(nx=1, ny=1, nz=100000, na=8, nb=8)
+    assert g["nx"] * g["ny"] * g["nz"] <= MAX_VOXELS
+    rc = L.mcsart_projection_noalloc(None, 16, 16, 0.3, *_args(g))
+    assert rc == _lib.ERR_INVALID_ARGUMENT
+    assert "nz must be at most 65535" in L.mcsart_last_error().decode()
