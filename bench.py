@@ -55,6 +55,10 @@ def parse():
     ap.add_argument("--profile-steps", type=int, default=0,
                     help="only run this many untimed steps inside the NVTX range "
                          "'mcsart_step' (for a profiler's launch list) and exit")
+    ap.add_argument("--kernel-case", default="", choices=["", "fp", "bp", "warp"],
+                    help="only time single calls of one kernel at the workload's size "
+                         "(projector, backprojector or warp through the C ABI, CUDA events, "
+                         "--steps calls after --warmup) and exit")
     return ap.parse_args()
 
 
@@ -203,14 +207,18 @@ def cpu_sample(p, proj_host, views: int, threads: int):
     O.set_num_threads(threads)
     nv = p.cfg.n_views
     views = max(2, min(views, nv))
-    it = dict(n_iter=2, op_iter=np.array([1, 0], np.int32), n_views=nv, outIter=1,
+    op = np.array([1, 0] if p.fields is not None else [1], np.int32)
+    it = dict(n_iter=len(op), op_iter=op, n_views=nv, outIter=1,
               volumes=p.volumes, flows=p.flows, angles=p.angles, **{"lambda": p.cfg.lam})
     t0 = time.perf_counter()
     O.aumisart(p.img0, proj_host, p.geo, it, p.fields, prec="cpu", view_lo=0, view_hi=views)
     dt = time.perf_counter() - t0
     # image pass: `views` views; motion pass: views-1 views (starts at view 1)
-    per_view = dt / (2 * views - 1)
-    t_iter = per_view * (nv + (nv - 1))
+    # motion: `views` image-pass views and views-1 DVF-pass views (it starts
+    # at view 1); static: `views` image-pass views
+    motion = p.fields is not None
+    per_view = dt / ((2 * views - 1) if motion else views)
+    t_iter = per_view * ((nv + (nv - 1)) if motion else nv)
     return dt, 1.0 / t_iter, views
 
 
@@ -337,6 +345,56 @@ def config_dict(p, args) -> dict:
 
 
 # -------------------------------------------------------------- GPU side
+def run_kernel_case(args, ctx, torch, stream):
+    """One kernel of the workload at its full size, on a smooth random volume
+    (the projector's and backprojector's memory traffic depends on the
+    geometry, not on the values): --steps calls timed with CUDA events on the
+    context's stream, after --warmup untimed ones."""
+    from mcsart_b200 import synthetic as S
+    cfg = S.CONFIGS[args.config]
+    g = S.geometry(cfg)
+    shape = (g["nz"], g["ny"], g["nx"])
+    gen = torch.Generator(device="cuda").manual_seed(5)
+    img = torch.rand(shape, device="cuda", generator=gen)
+    proj = torch.rand((g["nb"], g["na"]), device="cuda", generator=gen)
+    out_v = torch.empty_like(img)
+    out_p = torch.empty_like(proj)
+    geo = (g["SO"], g["SD"], g["da"], g["na"], g["ai"], g["db"], g["nb"], g["bi"], g["nx"],
+           g["ny"], g["nz"])
+    fields = ([torch.rand(shape, device="cuda", generator=gen) * 4 - 2 for _ in range(6)]
+              if args.kernel_case == "warp" else None)
+    angle = 0.3  # rays driven along x: the projector reads the volume's y-fastest copy
+
+    def call():
+        if args.kernel_case == "fp":
+            ctx.host_projection(out_p, img, angle, *geo)
+        elif args.kernel_case == "bp":
+            ctx.host_backprojection(out_v, proj, angle, *geo)
+        else:
+            ctx.host_deform(out_v, img, g["nx"], g["ny"], g["nz"], 0.7, -0.3, *fields)
+
+    for _ in range(max(args.warmup, 0)):
+        call()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    for e0, e1 in ev:
+        e0.record(stream)
+        call()
+        e1.record(stream)
+    torch.cuda.synchronize()
+    ms = [a.elapsed_time(b) for a, b in ev]
+    V, P = g["nx"] * g["ny"] * g["nz"], g["na"] * g["nb"]
+    abytes = {"fp": 4 * V + 4 * P, "bp": 4 * P + 4 * V, "warp": 4 * V + 24 * V + 4 * V}
+    print(json.dumps({"kernel_case": args.kernel_case, "config": args.config,
+                      "volume": [g["nx"], g["ny"], g["nz"]], "detector": [g["na"], g["nb"]],
+                      "calls": args.steps, "ms_median": float(np.median(ms)),
+                      "ms_min": float(np.min(ms)),
+                      "algorithmic_bytes": abytes[args.kernel_case],
+                      "note": "each call is one C-ABI call (the projector's includes the "
+                              "y-fastest copy of the volume for x-driven rays)"}), flush=True)
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -359,22 +417,30 @@ def main():
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     ctx = m.Context(local, stream=stream)
+    if args.kernel_case:
+        if rank == 0:
+            run_kernel_case(args, ctx, torch, stream)
+        ctx.close()
+        if dist_on:
+            dist.destroy_process_group()
+        return
     p, proj, fields = build_problem(ctx, torch, args.config, seed=rank)
     g = p.geo
     nv = p.cfg.n_views
     V = g["nx"] * g["ny"] * g["nz"]
-    op = np.array([1, 0], np.int32)
+    # motion workloads: an image pass and a DVF-update pass; static: an image pass
+    op = np.array([1, 0] if fields is not None else [1], np.int32)
     img = torch.zeros((g["nz"], g["ny"], g["nx"]), dtype=torch.float32, device="cuda")
-    F = torch.stack(fields).contiguous()
-    F0 = F.clone()
-    norm = torch.zeros(2 * nv, device="cuda")
+    F = torch.stack(fields).contiguous() if fields is not None else None
+    F0 = F.clone() if F is not None else None
+    norm = torch.zeros(len(op) * nv, device="cuda")
     resid = torch.zeros((nv, g["nb"], g["na"]), device="cuda")
     flush = torch.empty(256 * 2**20 // 4, dtype=torch.float32, device="cuda")
 
     def step(opts, img_t, F_t):
         ctx.aumisart_device(geo=g, n_views=nv, lambda_=p.cfg.lam, angles=p.angles,
                             volumes=p.volumes, flows=p.flows, img=img_t, proj=proj, fields=F_t,
-                            resid=resid, norm=norm, n_iter=2, op_iter=op, options=opts)
+                            resid=resid, norm=norm, n_iter=len(op), op_iter=op, options=opts)
 
     def timed(opts, steps, warmup, img_t, F_t, count_launches=False):
         for _ in range(warmup):
@@ -442,15 +508,15 @@ def main():
     pin = lambda a: torch.as_tensor(np.ascontiguousarray(a)).pin_memory().numpy()
     h_img = pin(np.zeros((g["nz"], g["ny"], g["nx"]), np.float32))
     h_proj = pin(proj.cpu().numpy())
-    h_fields = [pin(f.cpu().numpy()) for f in fields]
+    h_fields = [pin(f.cpu().numpy()) for f in fields] if fields is not None else [None] * 6
     o_img, o_ax = pin(np.zeros_like(h_img)), pin(np.zeros_like(h_img))
     o_proj = pin(np.zeros((nv, g["nb"], g["na"]), np.float32))
-    o_norm = pin(np.zeros(2 * nv, np.float32))
+    o_norm = pin(np.zeros(len(op) * nv, np.float32))
     errw = np.zeros(nv, np.float32)
 
     def e2e_step():
         ctx.host_AUMISART(o_img, o_proj, o_norm, o_ax, h_img, h_proj, g["nx"], g["ny"], g["nz"],
-                          g["na"], g["nb"], 1, nv, 2, op, g["da"], g["db"], g["ai"], g["bi"],
+                          g["na"], g["nb"], 1, nv, len(op), op, g["da"], g["db"], g["ai"], g["bi"],
                           g["SO"], g["SD"], 1.0, p.cfg.lam, p.volumes, p.flows, errw, p.angles,
                           *h_fields)
 
@@ -464,7 +530,8 @@ def main():
         e2e_step()
     e2e_total = max_over_ranks(time.perf_counter() - t0)
     e2e = {"value": args.steps / e2e_total * world, "unit": "iterations/s",
-           "h2d_bytes_per_step": int(h_img.nbytes + h_proj.nbytes + 6 * h_img.nbytes),
+           "h2d_bytes_per_step": int(h_img.nbytes + h_proj.nbytes +
+                                     (6 * h_img.nbytes if fields is not None else 0)),
            "d2h_bytes_per_step": int(o_img.nbytes + o_proj.nbytes + o_norm.nbytes + o_ax.nbytes),
            "api": "mcsart_aumisart (host pointers, pinned)"}
 
@@ -487,16 +554,16 @@ def main():
                                                     interp=m.INTERP_EXACT))):
             o = m.default_options(**kw)
             if o.storage == m.F32:
-                pr, Ft = proj, F0.clone()
+                pr, Ft = proj, (F0.clone() if F0 is not None else None)
             else:
                 dt = torch.bfloat16 if o.storage == m.BF16 else torch.float16
-                pr, Ft = proj.to(dt), F0.to(dt)
+                pr, Ft = proj.to(dt), (F0.to(dt) if F0 is not None else None)
             img2 = torch.zeros_like(img)
 
             def st(o=o, pr=pr, Ft=Ft, img2=img2):
                 ctx.aumisart_device(geo=g, n_views=nv, lambda_=p.cfg.lam, angles=p.angles,
                                     volumes=p.volumes, flows=p.flows, img=img2, proj=pr,
-                                    fields=Ft, resid=resid, norm=norm, n_iter=2, op_iter=op,
+                                    fields=Ft, resid=resid, norm=norm, n_iter=len(op), op_iter=op,
                                     options=o)
             for _ in range(2):
                 st()
@@ -522,12 +589,12 @@ def main():
                               img=torch.zeros_like(img), proj=prb,
                               fields=torch.stack(fb).contiguous() if fb else None))
         for _ in range(2):
-            ctx.batch_run(batch, n_iter=2, op_iter=op, options=drop_in)
+            ctx.batch_run(batch, n_iter=len(op), op_iter=op, options=drop_in)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for _ in range(xsteps):
-            ctx.batch_run(batch, n_iter=2, op_iter=op, options=drop_in)
+            ctx.batch_run(batch, n_iter=len(op), op_iter=op, options=drop_in)
         e1.record(stream)
         torch.cuda.synchronize()
         ext = max_over_ranks(e0.elapsed_time(e1) / 1000.0)
