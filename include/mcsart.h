@@ -164,6 +164,32 @@ int mcsart_projection_views(mcsart_ctx *ctx, float *d_proj, const float *d_img,
                             int na, float ai, float db, int nb, float bi, int nx, int ny,
                             int nz);
 
+/* -------------------------------------- mixed-precision kernel level */
+/* The engine's non-drop-in kernel forms, one call each, for measuring them
+ * against an FP64 reference.  No counterpart in the reference, whose
+ * kernels are FP32 only (src/cu_projection.cu, src/cu_backprojection.cu,
+ * src/cu_deform.cu).
+ *
+ * mcsart_projection_ex: the projection of a volume stored as `storage`
+ * (mcsart_dtype; FP32 accumulation), with projector summation fp_sum (0 the
+ * reference's order, as mcsart_projection; 1 per-slab partial sums; 2 the
+ * same with Kahan compensation) and geom64 = 1 for FP64 geometry (fp_sum 1
+ * or 2).  Output FP32. */
+int mcsart_projection_ex(mcsart_ctx *ctx, float *d_proj, const void *d_img, int storage,
+                         int fp_sum, int geom64, float angle, float SO, float SD, float da, int na,
+                         float ai, float db, int nb, float bi, int nx, int ny, int nz);
+/* mcsart_backprojection with geom64 = 1: voxel and detector boundary
+ * coordinates and overlap weights in FP64, terms accumulated in FP32
+ * (geom64 = 0 is mcsart_backprojection). */
+int mcsart_backprojection_ex(mcsart_ctx *ctx, float *d_img, const float *d_proj, int geom64,
+                             float angle, float SO, float SD, float da, int na, float ai,
+                             float db, int nb, float bi, int nx, int ny, int nz);
+/* mcsart_deform with the six DVF fields (contiguous, alpha_x .. beta_z) and
+ * the output stored as `storage`, and the warp model `interp`
+ * (mcsart_interp); d_img is FP32 and must not alias d_img1. */
+int mcsart_deform_ex(mcsart_ctx *ctx, void *d_img1, const float *d_img, int nx, int ny, int nz,
+                     float volume, float flow, const void *d_fields, int storage, int interp);
+
 /* ------------------------------------------------------------ drivers */
 /* replaces host_AUMISART, include/AUMISART.h:17 and :19 (src/AUMISART.cu:3,
  * :143).  Host pointers, the reference's argument list and order.  If alpha_x
@@ -201,6 +227,14 @@ typedef struct {
                          negated amplitudes (the reference); n > 0 = with the true
                          inverse of each view's displacement, n fixed-point steps
                          (mcsart_invert_dvf; FP32 storage, square slices; not a drop-in) */
+    int geom64;       /* 1: projector and backprojector geometry (source, detector and
+                         voxel boundary coordinates, overlap weights) in FP64 and the SART
+                         normalisation sums (row sums FP(1), column sums BP(FP(1))) in
+                         FP64; volume and residual terms still accumulate in FP32.  Needs
+                         fp_sum 1 or 2 (not a drop-in) */
+    int autotune;     /* 1: before the first run of a geometry (and storage type) that
+                         the context has no tuned launch shapes for, run
+                         mcsart_autotune; results are the same bits either way */
 } mcsart_options;
 void mcsart_default_options(mcsart_options *opt);
 
@@ -252,6 +286,27 @@ int mcsart_aumisart_fields(mcsart_ctx *ctx, float *h_outimg, float *h_outproj, f
 #define MCSART_BATCH_MAX 64
 int mcsart_batch_run(mcsart_ctx *ctx, const mcsart_problem *problems, int n_problems,
                      int n_iter, const int *h_op_iter, const mcsart_options *opt);
+
+/* ------------------------------------------------------------ tuning */
+/* Launch-shape autotuner, cached per geometry.  No counterpart in the
+ * reference, whose kernels have fixed launch shapes (src/cu_projection.cu:9,
+ * src/cu_backprojection.cu:46, src/cu_deform.cu:5).  Times the candidate
+ * shapes of the driver's per-view kernels (projector slab-group depth and
+ * blocks per SM, backprojector voxels per thread and rows per block, warp
+ * rows per thread) on a sample of the problem's views (an image pass and a
+ * DVF-update pass over up to 12 views, on copies of the image and fields;
+ * the problem's buffers are not changed) and caches the fastest for the
+ * problem's geometry and opt->storage.  Later driver runs of that geometry
+ * use them.  Every candidate gives the same bits. */
+int mcsart_autotune(mcsart_ctx *ctx, const mcsart_problem *prob, const mcsart_options *opt);
+/* The cached shapes of prob's geometry and `storage` as four variant indices
+ * (projector one-volume, projector three-volume, backprojector, warp; -1 =
+ * built-in): returns 1 and fills shapes[4], or 0 if none are cached. */
+int mcsart_tuning_get(mcsart_ctx *ctx, const mcsart_problem *prob, int storage, int *shapes);
+/* Write / read the context's tuning cache as a text file (one geometry per
+ * line); load returns the number of entries read. */
+int mcsart_tuning_save(mcsart_ctx *ctx, const char *path);
+int mcsart_tuning_load(mcsart_ctx *ctx, const char *path);
 
 /* ------------------------------------------ allocation-free projector */
 /* Largest volume, nx*ny*nz, that mcsart_projection_noalloc accepts: 2^22

@@ -36,7 +36,8 @@ class McsartError(RuntimeError):
 class Options(ctypes.Structure):
     _fields_ = [("storage", ctypes.c_int), ("interp", ctypes.c_int), ("use_graph", ctypes.c_int),
                 ("fp_sum", ctypes.c_int), ("fp_groups", ctypes.c_int), ("subset", ctypes.c_int),
-                ("dvf_inverse", ctypes.c_int)]
+                ("dvf_inverse", ctypes.c_int), ("geom64", ctypes.c_int),
+                ("autotune", ctypes.c_int)]
 
 
 class Problem(ctypes.Structure):
@@ -77,10 +78,17 @@ SIGNATURES = {
     "mcsart_diff": [_P, _P, _I, _I, _I, _I],
     "mcsart_snrm2": [_I, _P, ctypes.POINTER(ctypes.c_float)],
     "mcsart_projection_views": [_P, _P, _P, _I, _F, _F, _F, _I, _F, _F, _I, _F, _I, _I, _I],
+    "mcsart_projection_ex": [_P, _P, _I, _I, _I] + _GEO,
+    "mcsart_backprojection_ex": [_P, _P, _I] + _GEO,
+    "mcsart_deform_ex": [_P, _P, _I, _I, _I, _F, _F, _P, _I, _I],
     "mcsart_aumisart": [_P] * 6 + [_I] * 8 + [_P] + [_F] * 8 + [_P] * 4 + [_P] * 6,
     "mcsart_aumisart_fields": [_P] * 11 + [_I] * 8 + [_P] + [_F] * 8 + [_P] * 4 + [_P] * 6,
     "mcsart_aumisart_device": [ctypes.POINTER(Problem), _I, _P, ctypes.POINTER(Options)],
     "mcsart_batch_run": [ctypes.POINTER(Problem), _I, _I, _P, ctypes.POINTER(Options)],
+    "mcsart_autotune": [ctypes.POINTER(Problem), ctypes.POINTER(Options)],
+    "mcsart_tuning_get": [ctypes.POINTER(Problem), _I, ctypes.POINTER(ctypes.c_int)],
+    "mcsart_tuning_save": [ctypes.c_char_p],
+    "mcsart_tuning_load": [ctypes.c_char_p],
     "mcsart_set_stream": [_P],
     "mcsart_set_synchronous": [_I],
     "mcsart_set_interp": [_I],

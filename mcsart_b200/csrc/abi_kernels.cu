@@ -1,4 +1,6 @@
 // Kernel-level C ABI: one entry point per reference launcher (include/mcsart.h).
+#include <algorithm>
+
 #include "backprojector.cuh"
 #include "common.cuh"
 #include "elementwise.cuh"
@@ -367,4 +369,136 @@ MC_EXPORT int mcsart_snrm2(mcsart_ctx *ctx, int n, const float *d_x, float *h_re
     for (unsigned i = 0; i < blocks; i++) s += host[i];
     *h_result = (float)sqrt(s);
     return MCSART_OK;
+}
+
+// ------------------------------------------------- mixed-precision kernels
+namespace {
+
+template <typename VT>
+int projection_ex_typed(mcsart_ctx *ctx, float *d_proj, const VT *d_img, int fp_sum, int geom64,
+                        float angle, const Geom &g) {
+    const int64_t V = nvox(g.nx, g.ny, g.nz);
+    void *ws;
+    MC_TRY(workspace(ctx, "fp_volT_ex", V * sizeof(VT), &ws));
+    VT *imgT = (VT *)ws;
+    MC_LAUNCH(ctx, (transpose_kernel<VT, VT>), dim3(div_up(g.nx, 32), div_up(g.ny, 32), g.nz),
+              dim3(32, 8), 0, imgT, d_img, g.nx, g.ny);
+    FPArgs<VT, 1, VT> a{};
+    a.vol.std[0] = d_img;
+    a.vol.tr[0] = imgT;
+    a.g = g;
+    a.angle = angle;
+    a.mode = FP_PLAIN;
+    a.out = d_proj;
+    if (fp_sum == SUM_REF) {
+        MC_LAUNCH(ctx, (fp_ref_kernel<1, false, VT, VT>),
+                  dim3(div_up(g.na, FPC_COLS), div_up(g.nb, FPC_ROWS), 1), dim3(FPC_THREADS), 0,
+                  a);
+        return MCSART_OK;
+    }
+    const int groups = fp_auto_groups((int64_t)div_up(g.na, 32) * g.nb, std::max(g.nx, g.ny));
+    const dim3 grid(div_up(g.na, 32), g.nb, 1), block(32, groups);
+    const size_t smem = (size_t)groups * 2 * 32 * sizeof(float);
+    if (fp_sum == SUM_PLAIN && geom64)
+        MC_LAUNCH(ctx, (fp_kernel<1, false, SUM_PLAIN, VT, VT, true>), grid, block, smem, a);
+    else if (fp_sum == SUM_PLAIN)
+        MC_LAUNCH(ctx, (fp_kernel<1, false, SUM_PLAIN, VT, VT>), grid, block, smem, a);
+    else if (geom64)
+        MC_LAUNCH(ctx, (fp_kernel<1, false, SUM_KAHAN, VT, VT, true>), grid, block, smem, a);
+    else
+        MC_LAUNCH(ctx, (fp_kernel<1, false, SUM_KAHAN, VT, VT>), grid, block, smem, a);
+    return MCSART_OK;
+}
+
+template <typename FT>
+int deform_ex_typed(mcsart_ctx *ctx, FT *d_img1, const float *d_img, int nx, int ny, int nz,
+                    float volume, float flow, const FT *fields, int interp) {
+    const int64_t V = nvox(nx, ny, nz);
+    const Fields<FT> f{fields, fields + V, fields + 2 * V, fields + 3 * V, fields + 4 * V,
+                       fields + 5 * V};
+    const unsigned blocks = stream_blocks(V);
+    if (interp == MCSART_INTERP_TEXTURE) {
+        if (!ctx->driver) ctx->driver.reset(new DriverState());
+        TexVol &tv = ctx->driver->tv_deform;
+        MC_TRY(tv.ensure(nx, ny, nz));
+        MC_TRY(tv.upload(d_img, ctx->stream));
+        MC_LAUNCH(ctx, (deform_typed_kernel<SrcTex, FT>), blocks, 256, 0, d_img1, SrcTex{tv.tex},
+                  f, nx, ny, nz, volume, flow);
+    } else {
+        MC_LAUNCH(ctx, (deform_typed_kernel<SrcLinear<float>, FT>), blocks, 256, 0, d_img1,
+                  SrcLinear<float>{d_img}, f, nx, ny, nz, volume, flow);
+    }
+    return MCSART_OK;
+}
+
+}  // namespace
+
+MC_EXPORT int mcsart_projection_ex(mcsart_ctx *ctx, float *d_proj, const void *d_img,
+                                   int storage, int fp_sum, int geom64, float angle, float SO,
+                                   float SD, float da, int na, float ai, float db, int nb,
+                                   float bi, int nx, int ny, int nz) {
+    clear_error();
+    MC_TRY(validate_ctx(ctx));
+    MC_REQUIRE(d_proj && d_img, "d_proj and d_img must be non-NULL");
+    MC_REQUIRE(storage >= MCSART_F32 && storage <= MCSART_F16, "unknown storage type %d", storage);
+    MC_REQUIRE(fp_sum >= SUM_REF && fp_sum <= SUM_KAHAN, "fp_sum must be 0, 1 or 2");
+    MC_REQUIRE(geom64 == 0 || geom64 == 1, "geom64 must be 0 or 1");
+    MC_REQUIRE(geom64 == 0 || fp_sum != SUM_REF,
+               "FP64 geometry (geom64) needs a split summation projector (fp_sum 1 or 2)");
+    const Geom g = make_geom(SO, SD, da, na, ai, db, nb, bi, nx, ny, nz);
+    MC_TRY(validate_geom(g));
+    if (storage == MCSART_F32)
+        MC_TRY(projection_ex_typed(ctx, d_proj, (const float *)d_img, fp_sum, geom64, angle, g));
+    else if (storage == MCSART_BF16)
+        MC_TRY(projection_ex_typed(ctx, d_proj, (const __nv_bfloat16 *)d_img, fp_sum, geom64,
+                                   angle, g));
+    else
+        MC_TRY(projection_ex_typed(ctx, d_proj, (const __half *)d_img, fp_sum, geom64, angle, g));
+    return finish(ctx, "mcsart_projection_ex");
+}
+
+MC_EXPORT int mcsart_backprojection_ex(mcsart_ctx *ctx, float *d_img, const float *d_proj,
+                                       int geom64, float angle, float SO, float SD, float da,
+                                       int na, float ai, float db, int nb, float bi, int nx,
+                                       int ny, int nz) {
+    clear_error();
+    MC_TRY(validate_ctx(ctx));
+    MC_REQUIRE(d_proj && d_img, "d_proj and d_img must be non-NULL");
+    MC_REQUIRE(geom64 == 0 || geom64 == 1, "geom64 must be 0 or 1");
+    if (!geom64)
+        return mcsart_backprojection(ctx, d_img, d_proj, angle, SO, SD, da, na, ai, db, nb, bi,
+                                     nx, ny, nz);
+    const Geom g = make_geom(SO, SD, da, na, ai, db, nb, bi, nx, ny, nz);
+    MC_TRY(validate_geom(g));
+    BPArgs a{};
+    a.proj = d_proj;
+    a.g = g;
+    a.angle = angle;
+    a.out = d_img;
+    const dim3 grid(div_up(nx, 32), div_up(ny, BP_ROWS), div_up(nz, BP_NZ)), block(32, BP_ROWS);
+    MC_LAUNCH(ctx, (bp_kernel<1, BP_PLAIN, false, false, true>), grid, block, 0, a);
+    return finish(ctx, "mcsart_backprojection_ex");
+}
+
+MC_EXPORT int mcsart_deform_ex(mcsart_ctx *ctx, void *d_img1, const float *d_img, int nx, int ny,
+                               int nz, float volume, float flow, const void *d_fields, int storage,
+                               int interp) {
+    clear_error();
+    MC_TRY(validate_ctx(ctx));
+    MC_TRY(validate_dims(nx, ny, nz));
+    MC_REQUIRE(d_img1 && d_img && d_fields, "volume and field pointers must be non-NULL");
+    MC_REQUIRE(d_img1 != (const void *)d_img, "d_img1 must not alias d_img");
+    MC_REQUIRE(storage >= MCSART_F32 && storage <= MCSART_F16, "unknown storage type %d", storage);
+    MC_REQUIRE(interp == MCSART_INTERP_TEXTURE || interp == MCSART_INTERP_EXACT,
+               "unknown interpolation model %d", interp);
+    if (storage == MCSART_F32)
+        MC_TRY(deform_ex_typed(ctx, (float *)d_img1, d_img, nx, ny, nz, volume, flow,
+                               (const float *)d_fields, interp));
+    else if (storage == MCSART_BF16)
+        MC_TRY(deform_ex_typed(ctx, (__nv_bfloat16 *)d_img1, d_img, nx, ny, nz, volume, flow,
+                               (const __nv_bfloat16 *)d_fields, interp));
+    else
+        MC_TRY(deform_ex_typed(ctx, (__half *)d_img1, d_img, nx, ny, nz, volume, flow,
+                               (const __half *)d_fields, interp));
+    return finish(ctx, "mcsart_deform_ex");
 }

@@ -157,12 +157,12 @@ constexpr int BP_NZ = MCSART_BP_NZ;
 // detector rows take the general loop.
 constexpr int BP_WB = 4;
 
-// Overlap-weighted gather of one view for the BP_NZ voxels (ix, iy, z0 ..)
+// Overlap-weighted gather of one view for the NZ voxels (ix, iy, z0 ..)
 // of a thread: acc0 (and acc1 with K == 2) get the view's terms in the
 // reference's order (detector column outer, row inner, acc = fma(wa*wb, p,
 // acc), :150-168).  The column box and the column weights wa are shared by the
 // voxels of a thread, the row weights wb are computed once per voxel.
-template <int K, bool PROVEN>
+template <int K, bool PROVEN, int NZ = BP_NZ>
 __device__ __forceinline__ void bp_gather_view(const BPArgs &p, float angle, const float *proj,
                                                const float2 *pair, int ix, int iy, int z0,
                                                float *acc0, float *acc1) {
@@ -183,10 +183,10 @@ __device__ __forceinline__ void bp_gather_view(const BPArgs &p, float angle, con
     }
     // rows of each slice: first row, count (BP_WB + 1 = more than BP_WB),
     // row weights, box
-    int ib0[BP_NZ], nbk[BP_NZ];
-    float wb[BP_NZ][BP_WB], bmn[BP_NZ], bmx[BP_NZ];
+    int ib0[NZ], nbk[NZ];
+    float wb[NZ][BP_WB], bmn[NZ], bmx[NZ];
 #pragma unroll
-    for (int k = 0; k < BP_NZ; k++) {
+    for (int k = 0; k < NZ; k++) {
         nbk[k] = 0;
         ib0[k] = 0;
         bmn[k] = 0.0f;
@@ -214,7 +214,7 @@ __device__ __forceinline__ void bp_gather_view(const BPArgs &p, float angle, con
     for (int ia = ia0; (float)ia < alim; ia++) {
         const float wa = fminf(ia + 1.0f, col.amax) - fmaxf(ia + 0.0f, col.amin);
 #pragma unroll
-        for (int k = 0; k < BP_NZ; k++) {
+        for (int k = 0; k < NZ; k++) {
             if (nbk[k] <= BP_WB) {
 #pragma unroll
                 for (int j = 0; j < BP_WB; j++) {
@@ -249,34 +249,98 @@ __device__ __forceinline__ void bp_gather_view(const BPArgs &p, float angle, con
     }
 }
 
+// FP64 geometry (options.geom64): the footprint of bp_column / bp_rows
+// (src/cu_backprojection.cu:66-168) with every coordinate, box edge and
+// overlap weight in FP64 and the rotation by the FP64 sine and cosine of the
+// angle; the projection's terms (K == 1) or the residual's (K == 2) are
+// accumulated in FP32 (acc0), the normaliser's (the projection of a
+// ones-volume, the SART column sum; K == 2) in FP64 (acc1).  Same order of
+// terms as bp_gather_view.
+template <int K, int NZ = BP_NZ>
+__device__ __forceinline__ void bp_gather_view64(const BPArgs &p, float angle, const float *proj,
+                                                 const float2 *pair, int ix, int iy, int z0,
+                                                 float *acc0, double *acc1) {
+    const Geom &g = p.g;
+    const double SO = g.SO, SD = g.SD, da = g.da, db = g.db;
+    double sphi, cphi;
+    sincos((double)angle, &sphi, &cphi);
+    const double xc = (double)ix - g.nx / 2 + 0.5, yc = (double)iy - g.ny / 2 + 0.5;
+    const double t = xc * cphi + yc * sphi, u = -xc * sphi + yc * cphi;
+    const double rl = SD / (t - 0.5 + SO), rr = SD / (t + 0.5 + SO), r0 = SD / (t + SO);
+    const double all = rl * (u - 0.5), alr = rl * (u + 0.5);
+    const double arr = rr * (u + 0.5), arl = rr * (u - 0.5), at = r0 * u;
+    const double amax = fmax(fmax(fmax(all, arr), fmax(alr, arl)), at) / da - g.ai + 0.5;
+    const double amin = fmin(fmin(fmin(all, arr), fmin(alr, arl)), at) / da - g.ai + 0.5;
+    const int ia0 = max(0, (int)floor(fmax(amin, -1.0)));
+    const int ia1 = (int)ceil(fmin(amax, (double)g.na));  // columns ia < ia1
+#pragma unroll
+    for (int k = 0; k < NZ; k++) {
+        const int iz = z0 + k;
+        if (iz >= g.nz) continue;
+        const double zc = (double)iz - g.nz / 2 + 0.5;
+        const double bl = rl * zc, br = rr * zc, bt = r0 * (zc + 0.5), bb = r0 * (zc - 0.5);
+        const double bmax = fmax(fmax(bl, br), fmax(bt, bb)) / db - g.bi + 0.5;
+        const double bmin = fmin(fmin(bl, br), fmin(bt, bb)) / db - g.bi + 0.5;
+        const int ib0 = max(0, (int)floor(fmax(bmin, -1.0)));
+        const int ib1 = (int)ceil(fmin(bmax, (double)g.nb));
+        for (int ia = ia0; ia < ia1; ia++) {
+            const double wa = fmin(ia + 1.0, amax) - fmax((double)ia, amin);
+            for (int ib = ib0; ib < ib1; ib++) {
+                const double w = wa * (fmin(ib + 1.0, bmax) - fmax((double)ib, bmin));
+                if (K == 1) {
+                    acc0[k] = __fmaf_rn((float)w, __ldg(proj + ia + (int64_t)ib * g.na), acc0[k]);
+                } else {
+                    const float2 v = __ldg(pair + ia + (int64_t)ib * g.na);
+                    acc0[k] = __fmaf_rn((float)w, v.x, acc0[k]);
+                    acc1[k] = fma(w, (double)v.y, acc1[k]);
+                }
+            }
+        }
+    }
+}
+
 // blockDim = (32, BP_ROWS); each thread backprojects the BP_NZ voxels
 // (ix, iy, z0 .. z0 + BP_NZ - 1), z0 = blockIdx.z * BP_NZ, for every view of
 // the launch.
 // MULTI = false: one view (the reference's loop); the view loop and the
 // per-view outputs exist only in the ordered-subset instantiation, so that
 // the single-view kernel keeps its registers (and resident blocks).
-template <int K, int MODE, bool MULTI = false, bool PROVEN = false>
+// GEO64: FP64 geometry and normaliser (bp_gather_view64; one view).
+// NZ (voxels per thread along z) and ROWS (voxel rows per block) are the
+// launch shape the driver's tuning may choose; every shape gives the same
+// bits (each voxel's terms and their order do not depend on it).
+template <int K, int MODE, bool MULTI = false, bool PROVEN = false, bool GEO64 = false,
+          int NZ = BP_NZ, int ROWS = BP_ROWS>
 __global__ void __launch_bounds__(256, MCSART_BP_MINBLOCKS) bp_kernel(const BPArgs p) {
-    __shared__ float tile[BP_NZ][BP_ROWS][33];
+    __shared__ float tile[NZ][ROWS][33];
     const Geom &g = p.g;
     const int tx = threadIdx.x, ty = threadIdx.y;
-    const int x0 = blockIdx.x * 32, y0 = blockIdx.y * BP_ROWS, z0 = blockIdx.z * BP_NZ;
+    const int x0 = blockIdx.x * 32, y0 = blockIdx.y * ROWS, z0 = blockIdx.z * NZ;
     const int ix = x0 + tx, iy = y0 + ty;
     const bool active = ix < g.nx && iy < g.ny;
     const int64_t plane = (int64_t)g.nx * g.ny, V = plane * g.nz, NP = (int64_t)g.na * g.nb;
     const int nv = MULTI ? p.n_views : 1;
 
-    float qsum[BP_NZ];
+    float qsum[NZ];
 #pragma unroll
-    for (int k = 0; k < BP_NZ; k++) qsum[k] = 0.0f;
+    for (int k = 0; k < NZ; k++) qsum[k] = 0.0f;
     for (int v = 0; v < nv; v++) {
-        float acc0[BP_NZ], acc1[BP_NZ];
+        float acc0[NZ], acc1[NZ];
 #pragma unroll
-        for (int k = 0; k < BP_NZ; k++) { acc0[k] = 0.0f; acc1[k] = 0.0f; }
+        for (int k = 0; k < NZ; k++) { acc0[k] = 0.0f; acc1[k] = 0.0f; }
         const float angle = MULTI ? p.angles[v] : p.angle;
-        if (active) bp_gather_view<K, PROVEN>(p, angle, p.proj, p.pair + v * NP, ix, iy, z0, acc0, acc1);
+        double acc64[NZ];
+        if (GEO64) {
+            static_assert(!GEO64 || !MULTI, "FP64 geometry: one view per launch");
 #pragma unroll
-        for (int k = 0; k < BP_NZ; k++) {
+            for (int k = 0; k < NZ; k++) acc64[k] = 0.0;
+            if (active) bp_gather_view64<K, NZ>(p, angle, p.proj, p.pair, ix, iy, z0, acc0, acc64);
+        } else if (active) {
+            bp_gather_view<K, PROVEN, NZ>(p, angle, p.proj, p.pair + v * NP, ix, iy, z0, acc0,
+                                          acc1);
+        }
+#pragma unroll
+        for (int k = 0; k < NZ; k++) {
             const int iz = z0 + k;
             if (!(active && iz < g.nz)) continue;
             const int64_t id = ix + (int64_t)iy * g.nx + iz * plane;
@@ -284,7 +348,8 @@ __global__ void __launch_bounds__(256, MCSART_BP_MINBLOCKS) bp_kernel(const BPAr
                 p.out[id] = acc0[k];
                 continue;
             }
-            float q = acc0[k] / acc1[k];            // cu_division.cu:20
+            float q = GEO64 ? (float)((double)acc0[k] / acc64[k])
+                            : acc0[k] / acc1[k];    // cu_division.cu:20
             if (isnan(q) || isinf(q)) q = 0.0f;     // :21-24
             if (MODE == BP_DIV) {
                 if (p.out) p.out[id + v * V] = q;
@@ -297,7 +362,7 @@ __global__ void __launch_bounds__(256, MCSART_BP_MINBLOCKS) bp_kernel(const BPAr
     }
     if (MODE != BP_DIV_ADD) return;
 #pragma unroll
-    for (int k = 0; k < BP_NZ; k++) {
+    for (int k = 0; k < NZ; k++) {
         const int iz = z0 + k;
         float val = 0.0f;
         if (active && iz < g.nz) {
@@ -309,13 +374,13 @@ __global__ void __launch_bounds__(256, MCSART_BP_MINBLOCKS) bp_kernel(const BPAr
     }
     if (p.outT != nullptr) {
         __syncthreads();
-        // transposed store outT[iy + ix*ny + iz*nx*ny]: BP_ROWS consecutive iy per ix
+        // transposed store outT[iy + ix*ny + iz*nx*ny]: ROWS consecutive iy per ix
         const int t = ty * 32 + tx;
-        const int lx = t / BP_ROWS, ly = t % BP_ROWS;
+        const int lx = t / ROWS, ly = t % ROWS;
         const int ixT = x0 + lx, iyT = y0 + ly;
         if (ixT < g.nx && iyT < g.ny) {
 #pragma unroll
-            for (int k = 0; k < BP_NZ; k++) {
+            for (int k = 0; k < NZ; k++) {
                 const int iz = z0 + k;
                 if (iz < g.nz) p.outT[iyT + (int64_t)ixT * g.ny + iz * plane] = tile[k][ly][lx];
             }

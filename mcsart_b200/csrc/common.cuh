@@ -49,6 +49,17 @@ int check_launch(const char *what);
 
 struct DriverState;  // sart.cu
 
+// Launch shapes of the driver's per-view kernels (mcsart_autotune).  Each
+// field indexes the variant table of its kernel (tuning.cu); -1 selects the
+// built-in choice.  Every variant computes every ray and voxel with the same
+// operations in the same order, so the results do not depend on the choice.
+struct Tuning {
+    int fp1 = -1;   // one-volume projector (image passes): slab group depth, blocks per SM
+    int fp3 = -1;   // three-volume projector (DVF-update passes)
+    int bp = -1;    // backprojector: voxels per thread along z, voxel rows per block
+    int warp = -1;  // image-pass warps: voxel rows per thread
+};
+
 }  // namespace mcsart
 
 struct mcsart_ctx {
@@ -85,6 +96,11 @@ struct mcsart_ctx {
     std::vector<std::unique_ptr<mcsart_ctx>> lanes;
     std::vector<cudaEvent_t> lane_done;
     cudaEvent_t batch_start = nullptr;
+    // tuned launch shapes per geometry and storage type (mcsart_autotune,
+    // mcsart_tuning_load), keyed by tuning_key()
+    std::map<std::string, mcsart::Tuning> tuning;
+    // set while the tuner times a trial: the shapes every launch uses
+    const mcsart::Tuning *tuning_override = nullptr;
     ~mcsart_ctx();
 };
 
@@ -174,15 +190,18 @@ int validate_geom(const Geom &g);
 int validate_dims(int nx, int ny, int nz);
 
 // -------------------------------------------------------- storage types
+// Loads through the read-only data cache: every array read with ldv is
+// either not written during the kernel or read and written at one index by
+// one thread only.
 template <typename T> __device__ __forceinline__ float ldv(const T *p, int64_t i);
 template <> __device__ __forceinline__ float ldv<float>(const float *p, int64_t i) {
     return __ldg(p + i);
 }
 template <> __device__ __forceinline__ float ldv<__nv_bfloat16>(const __nv_bfloat16 *p, int64_t i) {
-    return __bfloat162float(p[i]);
+    return __bfloat162float(__ldg(p + i));
 }
 template <> __device__ __forceinline__ float ldv<__half>(const __half *p, int64_t i) {
-    return __half2float(p[i]);
+    return __half2float(__ldg(p + i));
 }
 // A storage-type value as float (a value, not a load).
 __device__ __forceinline__ float tof(float v) { return v; }

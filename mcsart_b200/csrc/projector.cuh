@@ -232,6 +232,119 @@ __device__ __forceinline__ void ray_slabs(const RayGeom &r, const FPVolumes<VT, 
     sw = accw;
 }
 
+// ------------------------------------------------------------------------
+// FP64 geometry (options.geom64, with the split summation modes): the same
+// footprint formulas as ray_geom / ray_slabs (src/cu_projection.cu:23-144),
+// every boundary coordinate and overlap weight in FP64; the volume terms
+// v * w are accumulated in FP32 (plainly or Kahan-compensated), the weight
+// sum (the projection of a ones-volume, the SART row normaliser) in FP64.
+struct RayGeom64 {
+    double r0, r1, r2, r3, rz0, rz1;
+    double u_off, u_half, d_half, src_d;
+    int nd, nu;
+    bool xdrive;
+};
+
+__device__ __forceinline__ RayGeom64 ray_geom64(double cphi, double sphi, int ia, int ib,
+                                                const Geom &g) {
+    const double SO = g.SO, SD = g.SD, da = g.da, db = g.db;
+    const double x1 = -SO * cphi, y1 = -SO * sphi;  // :25-26
+    const double x20 = SD - SO, y20 = ((double)ia + (double)g.ai) * da;
+    const double x2 = x20 * cphi - y20 * sphi, y2 = y20 * cphi + x20 * sphi;
+    const double z2 = ((double)ib + (double)g.bi) * db;
+    const double x21 = x2 - x1, y21 = y2 - y1;
+    RayGeom64 r;
+    r.xdrive = fabs(x21) > fabs(y21);  // :39
+    const double hda = da / 2.0, hdb = db / 2.0;
+    const double xl = x21 - hda * sphi, xr = x21 + hda * sphi;
+    const double yl = y21 - hda * cphi, yr = y21 + hda * cphi;
+    const double zl = z2 - hdb, zr = z2 + hdb;
+    if (r.xdrive) {
+        r.r0 = yl / xl; r.r1 = yl / xr; r.r2 = yr / xl; r.r3 = yr / xr;
+        r.rz0 = zl / x21; r.rz1 = zr / x21;
+        r.u_off = y1; r.u_half = (double)(g.ny / 2);
+        r.d_half = (double)g.nx / 2.0; r.src_d = x1;
+        r.nd = g.nx; r.nu = g.ny;
+    } else {
+        r.r0 = xl / yl; r.r1 = xl / yr; r.r2 = xr / yl; r.r3 = xr / yr;
+        r.rz0 = zl / y21; r.rz1 = zr / y21;
+        r.u_off = x1; r.u_half = (double)(g.nx / 2);
+        r.d_half = (double)g.ny / 2.0; r.src_d = y1;
+        r.nd = g.ny; r.nu = g.nx;
+    }
+    return r;
+}
+
+// Slabs [d0, d1) of one ray with FP64 geometry: s[k] (FP32 sums of the
+// volumes' terms) and sw (FP64 sum of the weights).
+template <int K, bool ONES, int SUM, typename VT>
+__device__ __forceinline__ void ray_slabs64(const RayGeom64 &r, const FPVolumes<VT, K> &v,
+                                            const Geom &g, int d0, int d1, float *s, double &sw) {
+    const VT *base[K];
+    int64_t su, sd;
+    const int64_t sz = (int64_t)g.nx * g.ny;
+    if (r.xdrive && v.tr[0] != nullptr) {
+#pragma unroll
+        for (int k = 0; k < K; k++) base[k] = v.tr[k];
+        su = 1; sd = g.ny;
+    } else {
+#pragma unroll
+        for (int k = 0; k < K; k++) base[k] = v.std[k];
+        if (r.xdrive) { su = g.nx; sd = 1; } else { su = 1; sd = g.nx; }
+    }
+    const double z_half = (double)(g.nz / 2);
+    float acc[K], cmp[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) { acc[k] = 0.0f; cmp[k] = 0.0f; }
+    double accw = 0.0;
+    for (int d = d0; d < d1; d++) {
+        const double dc = ((double)d + 0.5) - r.d_half - r.src_d;  // :52 / :105
+        const double c0 = r.r0 * dc + r.u_off + r.u_half, c1 = r.r1 * dc + r.u_off + r.u_half;
+        const double c2 = r.r2 * dc + r.u_off + r.u_half, c3 = r.r3 * dc + r.u_off + r.u_half;
+        const double ui1 = fmin(fmin(c0, c1), fmin(c2, c3));
+        const double ui2 = fmax(fmax(c0, c1), fmax(c2, c3));
+        const double cz0 = r.rz0 * dc + z_half, cz1 = r.rz1 * dc + z_half;  // :71-77
+        const double zi1 = fmin(cz0, cz1), zi2 = fmax(cz0, cz1);
+        // loop bounds clamped to the volume before the integer conversion
+        const int u_lo = max(0, (int)floor(fmax(ui1, -1.0)));
+        const int u_hi = min(r.nu - 1, (int)floor(fmin(ui2, (double)r.nu)));
+        const int z_lo = max(0, (int)floor(fmax(zi1, -1.0)));
+        const int z_hi = min(g.nz - 1, (int)floor(fmin(zi2, (double)g.nz)));
+        if (u_lo > u_hi || z_lo > z_hi) continue;
+        const double du = ui2 - ui1, dz = zi2 - zi1;
+        float ss[K];
+#pragma unroll
+        for (int k = 0; k < K; k++) ss[k] = 0.0f;
+        for (int u = u_lo; u <= u_hi; u++) {
+            const double wu = (fmin(u + 1.0, ui2) - fmax((double)u, ui1)) / du;  // :83 / :136
+            const int64_t row = (int64_t)u * su + (int64_t)d * sd;
+            for (int z = z_lo; z <= z_hi; z++) {
+                const double wz = (fmin(z + 1.0, zi2) - fmax((double)z, zi1)) / dz;  // :86 / :139
+                const double w = wu * wz;
+                const float wf = (float)w;
+                const int64_t a = row + (int64_t)z * sz;
+#pragma unroll
+                for (int k = 0; k < K; k++) ss[k] = __fmaf_rn(ldv(base[k], a), wf, ss[k]);
+                if (ONES) accw += w;
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            if (SUM == SUM_KAHAN) {
+                const float y = ss[k] - cmp[k];
+                const float t = acc[k] + y;
+                cmp[k] = (t - acc[k]) - y;
+                acc[k] = t;
+            } else {
+                acc[k] += ss[k];
+            }
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < K; k++) s[k] = acc[k];
+    sw = accw;
+}
+
 template <typename VT, int K, typename MT = VT> struct FPArgs {
     FPVolumes<VT, K> vol;
     Geom g;
@@ -644,11 +757,12 @@ inline bool fp_one_wave(const mcsart_ctx *ctx, unsigned bx, unsigned by) {
 // is resident at once (fp_one_wave), where the register budget costs no
 // occupancy.
 constexpr int FPC_MIN_BLOCKS_K1 = 6;
+// MINB: resident blocks per SM the register budget must allow (the launch
+// shape the driver's tuning may choose, with G; every choice gives the same
+// bits).
 template <int K, bool ONES, typename VT, typename MT = VT, bool MULTI = false,
-          int G = fp_group<K>()>
-__global__ void __launch_bounds__(FPC_THREADS, (K == 1 && G == 2) ? FPC_MIN_BLOCKS_K1
-                                                                   : FPC_MIN_BLOCKS)
-    fp_ref_kernel(const FPArgs<VT, K, MT> p) {
+          int G = fp_group<K>(), int MINB = (K == 1 && G == 2) ? FPC_MIN_BLOCKS_K1 : FPC_MIN_BLOCKS>
+__global__ void __launch_bounds__(FPC_THREADS, MINB) fp_ref_kernel(const FPArgs<VT, K, MT> p) {
     __shared__ SlabC sm_c[FPC_CHUNK][FPC_COLS];
     __shared__ double2 sm_norm[FPC_THREADS / 32];
     const Geom &g = p.g;
@@ -775,30 +889,45 @@ __global__ void __launch_bounds__(FPC_THREADS, (K == 1 && G == 2) ? FPC_MIN_BLOC
 // 8 rows per block, gridDim (ceil(na/32), ceil(nb/8), views).  Split modes:
 // blockDim (32, groups), threadIdx.y = slab group of the same 32 rays,
 // gridDim (ceil(na/32), nb, views).
-template <int K, bool ONES, int SUM, typename VT, typename MT = VT>
+// GEO64: FP64 geometry and weight sum (ray_geom64 / ray_slabs64); split
+// summation modes only.
+template <int K, bool ONES, int SUM, typename VT, typename MT = VT, bool GEO64 = false>
 __global__ void __launch_bounds__(256) fp_kernel(const FPArgs<VT, K, MT> p) {
+    static_assert(!GEO64 || SUM != SUM_REF, "FP64 geometry needs a split summation mode");
     constexpr int NS = K + (ONES ? 1 : 0);
     extern __shared__ float sm_fp[];  // split modes: [groups][NS][32]
     __shared__ double2 sm_norm[8];
+    __shared__ double sm_w64[GEO64 ? 8 : 1][32];  // GEO64: the groups' FP64 weight sums
     const int lane = threadIdx.x;
     const Geom &g = p.g;
     const int ia = blockIdx.x * 32 + lane;
     const int ib = (SUM == SUM_REF) ? blockIdx.y * 8 + threadIdx.y : blockIdx.y;
     const bool active = ia < g.na && ib < g.nb;
     float s[K], sw = 0.0f;
+    double sw64 = 0.0;
 #pragma unroll
     for (int k = 0; k < K; k++) s[k] = 0.0f;
     if (active) {
         const float angle = p.angles ? p.angles[blockIdx.z] : p.angle;
-        const float cphi = cosf(angle), sphi = sinf(angle);  // :23-24
-        const RayGeom r = ray_geom(cphi, sphi, ia, ib, g);
-        if (SUM == SUM_REF) {
-            ray_slabs<K, ONES, SUM, VT>(r, p.vol, g, 0, r.nd, s, sw);
-        } else {
+        if (GEO64) {
+            double sd, cd;
+            sincos((double)angle, &sd, &cd);
+            const RayGeom64 r = ray_geom64(cd, sd, ia, ib, g);
             const int groups = blockDim.y, grp = threadIdx.y;
             const int per = (r.nd + groups - 1) / groups;
             const int d0 = grp * per, d1 = min(r.nd, d0 + per);
-            ray_slabs<K, ONES, SUM, VT>(r, p.vol, g, d0, d1, s, sw);
+            ray_slabs64<K, ONES, SUM, VT>(r, p.vol, g, d0, d1, s, sw64);
+        } else {
+            const float cphi = cosf(angle), sphi = sinf(angle);  // :23-24
+            const RayGeom r = ray_geom(cphi, sphi, ia, ib, g);
+            if (SUM == SUM_REF) {
+                ray_slabs<K, ONES, SUM, VT>(r, p.vol, g, 0, r.nd, s, sw);
+            } else {
+                const int groups = blockDim.y, grp = threadIdx.y;
+                const int per = (r.nd + groups - 1) / groups;
+                const int d0 = grp * per, d1 = min(r.nd, d0 + per);
+                ray_slabs<K, ONES, SUM, VT>(r, p.vol, g, d0, d1, s, sw);
+            }
         }
     }
     if (SUM != SUM_REF) {
@@ -806,6 +935,7 @@ __global__ void __launch_bounds__(256) fp_kernel(const FPArgs<VT, K, MT> p) {
 #pragma unroll
         for (int k = 0; k < K; k++) sm_fp[(grp * NS + k) * 32 + lane] = s[k];
         if (ONES) sm_fp[(grp * NS + K) * 32 + lane] = sw;
+        if (GEO64) sm_w64[grp][lane] = sw64;
         __syncthreads();
         if (grp != 0) return;
         // fixed-order combination of the slab groups
@@ -813,7 +943,9 @@ __global__ void __launch_bounds__(256) fp_kernel(const FPArgs<VT, K, MT> p) {
 #pragma unroll
             for (int k = 0; k < K; k++) s[k] += sm_fp[(q * NS + k) * 32 + lane];
             if (ONES) sw += sm_fp[(q * NS + K) * 32 + lane];
+            if (GEO64) sw64 += sm_w64[q][lane];
         }
+        if (GEO64) sw = (float)sw64;
     }
     const int64_t pix = ia + (int64_t)ib * g.na;
     double nb2 = 0.0, nr2 = 0.0;

@@ -64,18 +64,6 @@ void PassGraph::release() {
 
 enum PassKind { PASS_IMAGE_STATIC = 1, PASS_IMAGE_MC = 2, PASS_MOTION = 3 };
 
-struct Problem {
-    Geom g;
-    int n_views;
-    float lambda;
-    const float *angles, *volumes, *flows;  // host, n_views each
-    float *img;                             // device, FP32
-    const void *proj;                       // device, storage type, n_views*na*nb
-    void *fields;                           // device, storage type, 6 volumes
-    bool motion_model;                      // overload 2
-    float *resid;                           // device FP32 or nullptr
-};
-
 template <typename ST, int INTERP, int SUM> struct Runner {
     mcsart_ctx *ctx;
     DriverState &S;
@@ -87,9 +75,11 @@ template <typename ST, int INTERP, int SUM> struct Runner {
     int inv_iters = 0;  // fixed-point steps of the true DVF inverse (0: negated amplitudes)
     int cols_view = -1;  // view whose backprojector column data the last projector wrote
     std::vector<int> views_img, views_mot;
+    Tuning tune;  // launch shapes (variant indices; -1 = built-in choice)
 
     Runner(mcsart_ctx *c, const Problem &p, const mcsart_options &o)
         : ctx(c), S(*c->driver), P(p), opt(o) {
+        tune = c->tuning_override ? *c->tuning_override : tuning_for(c, p.g, o.storage);
         V = nvox(P.g.nx, P.g.ny, P.g.nz);
         NP = (int64_t)P.g.na * P.g.nb;
         fp_bx = SUM == SUM_REF ? (int)div_up(P.g.na, FPC_COLS) : (int)div_up(P.g.na, 32);
@@ -176,12 +166,29 @@ template <typename ST, int INTERP, int SUM> struct Runner {
             a.bpcolA = S.bpcolA.as<float4>();
             a.bpcolB = S.bpcolB.as<float>();
         }
-        if (SUM == SUM_REF && K == 1 && fp_one_wave(ctx, fp_bx, fp_by)) {
-            // every block resident at once: deeper slab groups (fp_ref_kernel)
-            MC_LAUNCH(ctx, (fp_ref_kernel<K, ONES, VT, ST, false, 4>), grid, dim3(FPC_THREADS), 0,
-                      a);
+        if (SUM == SUM_REF && K == 1) {
+            // built-in: deeper slab groups when every block is resident at once
+            const int var = tune.fp1 >= 0 ? tune.fp1 : fp_one_wave(ctx, fp_bx, fp_by) ? 1 : 0;
+            if (var == 1)
+                MC_LAUNCH(ctx, (fp_ref_kernel<K, ONES, VT, ST, false, 4, 4>), grid,
+                          dim3(FPC_THREADS), 0, a);
+            else if (var == 2)
+                MC_LAUNCH(ctx, (fp_ref_kernel<K, ONES, VT, ST, false, 1, 8>), grid,
+                          dim3(FPC_THREADS), 0, a);
+            else
+                MC_LAUNCH(ctx, (fp_ref_kernel<K, ONES, VT, ST, false, 2, 6>), grid,
+                          dim3(FPC_THREADS), 0, a);
         } else if (SUM == SUM_REF) {
-            MC_LAUNCH(ctx, (fp_ref_kernel<K, ONES, VT, ST>), grid, dim3(FPC_THREADS), 0, a);
+            if (tune.fp3 == 1)
+                MC_LAUNCH(ctx, (fp_ref_kernel<K, ONES, VT, ST, false, 2, 4>), grid,
+                          dim3(FPC_THREADS), 0, a);
+            else
+                MC_LAUNCH(ctx, (fp_ref_kernel<K, ONES, VT, ST, false, 4, 4>), grid,
+                          dim3(FPC_THREADS), 0, a);
+        } else if (opt.geom64) {
+            const size_t smem = (size_t)groups * (K + 1) * 32 * sizeof(float);
+            MC_LAUNCH(ctx, (fp_kernel<K, ONES, SUM == SUM_REF ? SUM_PLAIN : SUM, VT, ST, true>),
+                      grid, dim3(32, groups), smem, a);
         } else {
             const size_t smem = (size_t)groups * (K + 1) * 32 * sizeof(float);
             MC_LAUNCH(ctx, (fp_kernel<K, ONES, SUM, VT, ST>), grid, dim3(32, groups), smem, a);
@@ -202,19 +209,41 @@ template <typename ST, int INTERP, int SUM> struct Runner {
             b.colA = S.bpcolA.as<float4>();
             b.colB = S.bpcolB.as<float>();
         }
-        const dim3 grid(div_up(P.g.nx, 32), div_up(P.g.ny, BP_ROWS), div_up(P.g.nz, BP_NZ)),
-            block(32, BP_ROWS);
+        ctx->label = mode == BP_DIV ? "bp_div" : "bp_div_add";
+        if (opt.geom64) {  // FP64 geometry and normaliser (no precomputed columns)
+            b.colA = nullptr;
+            b.colB = nullptr;
+            const dim3 grid(div_up(P.g.nx, 32), div_up(P.g.ny, BP_ROWS), div_up(P.g.nz, BP_NZ)),
+                block(32, BP_ROWS);
+            if (mode == BP_DIV)
+                MC_LAUNCH(ctx, (bp_kernel<2, BP_DIV, false, false, true>), grid, block, 0, b);
+            else
+                MC_LAUNCH(ctx, (bp_kernel<2, BP_DIV_ADD, false, false, true>), grid, block, 0, b);
+            return MCSART_OK;
+        }
+        switch (tune.bp) {  // voxels per thread along z x voxel rows per block
+            case 1: return launch_bp_shape<1, 4>(mode, b);
+            case 2: return launch_bp_shape<2, 8>(mode, b);
+            case 3: return launch_bp_shape<4, 4>(mode, b);
+            default: return launch_bp_shape<BP_NZ, BP_ROWS>(mode, b);
+        }
+    }
+
+    template <int NZ, int ROWS> int launch_bp_shape(int mode, const BPArgs &b) {
+        const dim3 grid(div_up(P.g.nx, 32), div_up(P.g.ny, ROWS), div_up(P.g.nz, NZ)),
+            block(32, ROWS);
         // the proven form skips the division range checks (bp_geom_proven)
         const bool proven = bp_geom_proven(P.g);
-        ctx->label = mode == BP_DIV ? "bp_div" : "bp_div_add";
         if (mode == BP_DIV && proven) {
-            MC_LAUNCH(ctx, (bp_kernel<2, BP_DIV, false, true>), grid, block, 0, b);
+            MC_LAUNCH(ctx, (bp_kernel<2, BP_DIV, false, true, false, NZ, ROWS>), grid, block, 0, b);
         } else if (mode == BP_DIV) {
-            MC_LAUNCH(ctx, (bp_kernel<2, BP_DIV>), grid, block, 0, b);
+            MC_LAUNCH(ctx, (bp_kernel<2, BP_DIV, false, false, false, NZ, ROWS>), grid, block, 0, b);
         } else if (proven) {
-            MC_LAUNCH(ctx, (bp_kernel<2, BP_DIV_ADD, false, true>), grid, block, 0, b);
+            MC_LAUNCH(ctx, (bp_kernel<2, BP_DIV_ADD, false, true, false, NZ, ROWS>), grid, block, 0,
+                      b);
         } else {
-            MC_LAUNCH(ctx, (bp_kernel<2, BP_DIV_ADD>), grid, block, 0, b);
+            MC_LAUNCH(ctx, (bp_kernel<2, BP_DIV_ADD, false, false, false, NZ, ROWS>), grid, block, 0,
+                      b);
         }
         return MCSART_OK;
     }
@@ -274,9 +303,51 @@ template <typename ST, int INTERP, int SUM> struct Runner {
     }
 
     dim3 tile_grid() const { return dim3(div_up(P.g.nx, 32), div_up(P.g.ny, 32), P.g.nz); }
-    // warp_fwd_kernel / warp_back_add_kernel: 32 x (8 * WARP_ROWS) tiles
-    dim3 warp_grid() const {
-        return dim3(div_up(P.g.nx, 32), div_up(P.g.ny, 8 * WARP_ROWS), P.g.nz);
+    // warp_fwd_kernel / warp_back_add_kernel: 32 x (8 * WR) tiles
+    template <int WR = WARP_ROWS> dim3 warp_grid() const {
+        return dim3(div_up(P.g.nx, 32), div_up(P.g.ny, 8 * WR), P.g.nz);
+    }
+
+    // The image pass's forward warp of the volume into a view's phase, in the
+    // tuned launch shape (voxel rows per thread).
+    template <int WR> int warp_fwd_shape(bool hw, float volume, float flow) {
+        const Geom &g = P.g;
+        const Fields<ST> f = fields();
+        ctx->label = "warp_fwd";
+        if (hw) {
+            MC_LAUNCH(ctx, (warp_fwd_kernel<SrcTex, ST, ST, WR>), warp_grid<WR>(), dim3(32, 8), 0,
+                      S.img1.as<ST>(), S.img1T.as<ST>(), SrcTex{S.tv_img.tex}, f, g.nx, g.ny,
+                      g.nz, volume, flow);
+        } else {
+            MC_LAUNCH(ctx, (warp_fwd_kernel<SrcLinear<float>, ST, ST, WR>), warp_grid<WR>(),
+                      dim3(32, 8), 0, S.img1.as<ST>(), S.img1T.as<ST>(), SrcLinear<float>{P.img},
+                      f, g.nx, g.ny, g.nz, volume, flow);
+        }
+        return MCSART_OK;
+    }
+    int warp_fwd(bool hw, float volume, float flow) {
+        switch (tune.warp) {
+            case 1: return warp_fwd_shape<1>(hw, volume, flow);
+            case 2: return warp_fwd_shape<4>(hw, volume, flow);
+            default: return warp_fwd_shape<WARP_ROWS>(hw, volume, flow);
+        }
+    }
+    // The backward warp of a view's correction and the update, tuned shape.
+    template <int WR>
+    int warp_back_shape(bool hw, cudaTextureObject_t tex, const float *lin, float ivolume,
+                        float iflow, float lam) {
+        const Geom &g = P.g;
+        const Fields<ST> f = fields();
+        ctx->label = "warp_back_add";
+        if (hw) {
+            MC_LAUNCH(ctx, (warp_back_add_kernel<SrcTex, ST, WR>), warp_grid<WR>(), dim3(32, 8), 0,
+                      P.img, S.tv_img.surf, SrcTex{tex}, f, g.nx, g.ny, g.nz, ivolume, iflow, lam);
+        } else {
+            MC_LAUNCH(ctx, (warp_back_add_kernel<SrcLinear<float>, ST, WR>), warp_grid<WR>(),
+                      dim3(32, 8), 0, P.img, (cudaSurfaceObject_t)0, SrcLinear<float>{lin}, f,
+                      g.nx, g.ny, g.nz, ivolume, iflow, lam);
+        }
+        return MCSART_OK;
     }
 
     int finalize_norms(const int *views_dev, int n) {
@@ -343,16 +414,11 @@ template <typename ST, int INTERP, int SUM> struct Runner {
         }
         const float ivolume = P.volumes[0] - P.volumes[v];  // :222
         const float iflow = P.flows[0] - P.flows[v];
-        ctx->label = "warp_back_add";
-        if (hw) {
-            MC_LAUNCH(ctx, (warp_back_add_kernel<SrcTex, ST>), warp_grid(), dim3(32, 8), 0, P.img,
-                      S.tv_img.surf, SrcTex{tex}, f, g.nx, g.ny, g.nz, ivolume, iflow, lam);
-        } else {
-            MC_LAUNCH(ctx, (warp_back_add_kernel<SrcLinear<float>, ST>), warp_grid(), dim3(32, 8),
-                      0, P.img, (cudaSurfaceObject_t)0, SrcLinear<float>{lin}, f, g.nx, g.ny,
-                      g.nz, ivolume, iflow, lam);
+        switch (tune.warp) {
+            case 1: return warp_back_shape<1>(hw, tex, lin, ivolume, iflow, lam);
+            case 2: return warp_back_shape<4>(hw, tex, lin, ivolume, iflow, lam);
+            default: return warp_back_shape<WARP_ROWS>(hw, tex, lin, ivolume, iflow, lam);
         }
-        return MCSART_OK;
     }
 
     // Ordered subset of kk > 1 views in the motion-compensated image pass:
@@ -371,10 +437,10 @@ template <typename ST, int INTERP, int SUM> struct Runner {
             ST *d = S.img1.as<ST>() + j * V, *dT = S.img1T.as<ST>() + j * V;
             ctx->label = "warp_fwd";
             if (hw) {
-                MC_LAUNCH(ctx, (warp_fwd_kernel<SrcTex, ST, ST>), warp_grid(), dim3(32, 8), 0, d,
+                MC_LAUNCH(ctx, (warp_fwd_kernel<SrcTex, ST, ST>), warp_grid<>(), dim3(32, 8), 0, d,
                           dT, SrcTex{S.tv_img.tex}, f, g.nx, g.ny, g.nz, volume, flow);
             } else {
-                MC_LAUNCH(ctx, (warp_fwd_kernel<SrcLinear<float>, ST, ST>), warp_grid(),
+                MC_LAUNCH(ctx, (warp_fwd_kernel<SrcLinear<float>, ST, ST>), warp_grid<>(),
                           dim3(32, 8), 0, d, dT, SrcLinear<float>{P.img}, f, g.nx, g.ny, g.nz,
                           volume, flow);
             }
@@ -420,16 +486,7 @@ template <typename ST, int INTERP, int SUM> struct Runner {
             const int v = views_img[k];
             const float volume = P.volumes[v] - P.volumes[0];   // :193
             const float flow = P.flows[v] - P.flows[0];
-            ctx->label = "warp_fwd";
-            if (hw) {
-                MC_LAUNCH(ctx, (warp_fwd_kernel<SrcTex, ST, ST>), warp_grid(), dim3(32, 8), 0,
-                          S.img1.as<ST>(), S.img1T.as<ST>(), SrcTex{S.tv_img.tex}, f, g.nx, g.ny,
-                          g.nz, volume, flow);
-            } else {
-                MC_LAUNCH(ctx, (warp_fwd_kernel<SrcLinear<float>, ST, ST>), warp_grid(),
-                          dim3(32, 8), 0, S.img1.as<ST>(), S.img1T.as<ST>(),
-                          SrcLinear<float>{P.img}, f, g.nx, g.ny, g.nz, volume, flow);
-            }
+            MC_TRY(warp_fwd(hw, volume, flow));
             MC_TRY((launch_fp<1, true, ST>(vol, v, k, FP_IMAGE)));
             if (hw)
                 MC_TRY(launch_bp(v, BP_DIV, nullptr, nullptr, S.tv_ratio.surf));
@@ -515,8 +572,9 @@ template <typename ST, int INTERP, int SUM> struct Runner {
             k.insert(k.end(), b, b + n);
         };
         // the storage type itself, not its size: BF16 and F16 are both 2 bytes
-        const int hdr[9] = {kind, opt.storage, INTERP, SUM, groups, (int)P.motion_model,
-                            (int)views_mot.size(), subset, inv_iters};
+        const int hdr[14] = {kind, opt.storage, INTERP, SUM, groups, (int)P.motion_model,
+                             (int)views_mot.size(), subset, inv_iters, opt.geom64,
+                             tune.fp1, tune.fp3, tune.bp, tune.warp};
         put(hdr, sizeof(hdr));
         put(views_img.data(), views_img.size() * sizeof(int));
         put(views_mot.data(), views_mot.size() * sizeof(int));
@@ -632,6 +690,10 @@ int validate_options(const mcsart_options &o) {
     MC_REQUIRE(o.dvf_inverse >= 0 && o.dvf_inverse <= 64, "dvf_inverse must be in [0, 64]");
     MC_REQUIRE(o.dvf_inverse == 0 || o.storage == MCSART_F32,
                "the true DVF inverse (dvf_inverse > 0) needs FP32 storage");
+    MC_REQUIRE(o.geom64 == 0 || o.geom64 == 1, "geom64 must be 0 or 1");
+    MC_REQUIRE(o.geom64 == 0 || o.fp_sum != SUM_REF,
+               "FP64 geometry (geom64) needs a split summation projector (fp_sum 1 or 2)");
+    MC_REQUIRE(o.autotune == 0 || o.autotune == 1, "autotune must be 0 or 1");
     return MCSART_OK;
 }
 
@@ -657,23 +719,22 @@ MC_EXPORT void mcsart_default_options(mcsart_options *opt) {
     opt->fp_groups = 0;
     opt->subset = 1;
     opt->dvf_inverse = 0;
+    opt->geom64 = 0;
+    opt->autotune = 0;
 }
 
-MC_EXPORT int mcsart_aumisart_device(mcsart_ctx *ctx, const mcsart_problem *prob, int n_iter,
-                                     const int *h_op_iter, const mcsart_options *opt_in) {
-    clear_error();
-    MC_TRY(validate_ctx(ctx));
-    MC_REQUIRE(prob, "problem is NULL");
-    mcsart_options opt;
-    if (opt_in) opt = *opt_in; else mcsart_default_options(&opt);
-    MC_TRY(validate_options(opt));
+// The driver's view of a device-resident problem (validated); overload 1
+// (no fields) gets the context's zero-initialised fields.
+static int prepare_problem(mcsart_ctx *ctx, const mcsart_problem *prob, const mcsart_options &opt,
+                           Problem &P) {
     Geom g;
     g.SO = prob->SO; g.SD = prob->SD; g.da = prob->da; g.ai = prob->ai; g.db = prob->db;
     g.bi = prob->bi; g.na = prob->na; g.nb = prob->nb; g.nx = prob->nx; g.ny = prob->ny;
     g.nz = prob->nz;
     MC_TRY(validate_geom(g));
-    MC_TRY(validate_iter(prob->n_views, n_iter, h_op_iter, prob->h_angles, prob->h_volumes,
-                         prob->h_flows));
+    MC_REQUIRE(prob->n_views > 0, "n_views must be positive");
+    MC_REQUIRE(prob->h_angles && prob->h_volumes && prob->h_flows,
+               "angles, volumes and flows must be non-NULL");
     MC_REQUIRE(prob->d_img && prob->d_proj, "d_img and d_proj must be non-NULL");
     MC_REQUIRE(opt.dvf_inverse == 0 || prob->d_fields == nullptr || prob->nx == prob->ny,
                "the true DVF inverse (dvf_inverse > 0) needs square slices (nx == ny)");
@@ -681,7 +742,7 @@ MC_EXPORT int mcsart_aumisart_device(mcsart_ctx *ctx, const mcsart_problem *prob
     DriverState &S = *ctx->driver;
     const int64_t V = nvox(g.nx, g.ny, g.nz);
     const size_t es = opt.storage == MCSART_F32 ? 4 : 2;
-    Problem P;
+    P = Problem();
     P.g = g;
     P.n_views = prob->n_views;
     P.lambda = prob->lambda;
@@ -699,11 +760,42 @@ MC_EXPORT int mcsart_aumisart_device(mcsart_ctx *ctx, const mcsart_problem *prob
         MC_CHECK_CUDA(cudaMemsetAsync(S.zero_fields.ptr, 0, 6 * V * es, ctx->stream));
         P.fields = S.zero_fields.ptr;
     }
+    return MCSART_OK;
+}
+
+MC_EXPORT int mcsart_aumisart_device(mcsart_ctx *ctx, const mcsart_problem *prob, int n_iter,
+                                     const int *h_op_iter, const mcsart_options *opt_in) {
+    clear_error();
+    MC_TRY(validate_ctx(ctx));
+    MC_REQUIRE(prob, "problem is NULL");
+    mcsart_options opt;
+    if (opt_in) opt = *opt_in; else mcsart_default_options(&opt);
+    MC_TRY(validate_options(opt));
+    MC_TRY(validate_iter(prob->n_views, n_iter, h_op_iter, prob->h_angles, prob->h_volumes,
+                         prob->h_flows));
+    Problem P;
+    MC_TRY(prepare_problem(ctx, prob, opt, P));
+    if (opt.autotune && !ctx->tuning.count(tuning_key(P.g, opt.storage)))
+        MC_TRY(autotune_problem(ctx, P, opt));
     if (prob->d_norm)
         MC_CHECK_CUDA(cudaMemsetAsync(prob->d_norm, 0, (size_t)n_iter * prob->n_views * sizeof(float),
                                       ctx->stream));
     MC_TRY(run_driver(ctx, P, n_iter, h_op_iter, prob->d_norm, opt));
     return finish(ctx, "mcsart_aumisart_device");
+}
+
+MC_EXPORT int mcsart_autotune(mcsart_ctx *ctx, const mcsart_problem *prob,
+                              const mcsart_options *opt_in) {
+    clear_error();
+    MC_TRY(validate_ctx(ctx));
+    MC_REQUIRE(prob, "problem is NULL");
+    mcsart_options opt;
+    if (opt_in) opt = *opt_in; else mcsart_default_options(&opt);
+    MC_TRY(validate_options(opt));
+    Problem P;
+    MC_TRY(prepare_problem(ctx, prob, opt, P));
+    MC_TRY(autotune_problem(ctx, P, opt));
+    return finish(ctx, "mcsart_autotune");
 }
 
 MC_EXPORT int mcsart_batch_run(mcsart_ctx *ctx, const mcsart_problem *problems,

@@ -6,6 +6,7 @@
 
 #include <cstdint>
 #include <map>
+#include <string>
 #include <vector>
 
 #include "common.cuh"
@@ -28,6 +29,31 @@ struct PassGraph {
     void release();
     ~PassGraph() { release(); }
 };
+
+// One reconstruction problem as the driver sees it.
+struct Problem {
+    Geom g;
+    int n_views;
+    float lambda;
+    const float *angles, *volumes, *flows;  // host, n_views each
+    float *img;                             // device, FP32
+    const void *proj;                       // device, storage type, n_views*na*nb
+    void *fields;                           // device, storage type, 6 volumes
+    bool motion_model;                      // overload 2
+    float *resid;                           // device FP32 or nullptr
+};
+
+// Runs n_iter passes of host_AUMISART's loop (sart.cu).
+int run_driver(mcsart_ctx *ctx, const Problem &P, int n_iter, const int *op_iter, float *norm_out,
+               const mcsart_options &opt);
+
+// Tuning cache key of a geometry and storage type, and the tuned launch
+// shapes for it (the built-in choices where none are cached) (tuning.cu).
+std::string tuning_key(const Geom &g, int storage);
+Tuning tuning_for(const mcsart_ctx *ctx, const Geom &g, int storage);
+// Times the variants of the driver's kernels on a sample of P's views and
+// caches the fastest for P's geometry (tuning.cu).
+int autotune_problem(mcsart_ctx *ctx, const Problem &P, const mcsart_options &opt);
 
 struct DriverState {
     // working volumes of the passes

@@ -73,6 +73,19 @@ static __global__ void __launch_bounds__(256) deform_kernel(float *out, const SR
         out[id] = warp_sample(src, f, id, nx, ny, nz, volume, flow);
 }
 
+// deform_kernel with fields and output in a storage type FT (the kernel-level
+// form of the driver's 16-bit warps).
+template <typename SRC, typename FT>
+static __global__ void __launch_bounds__(256) deform_typed_kernel(FT *out, const SRC src,
+                                                                  Fields<FT> f, int nx, int ny,
+                                                                  int nz, float volume,
+                                                                  float flow) {
+    const int64_t n = nvox(nx, ny, nz);
+    for (int64_t id = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; id < n;
+         id += (int64_t)gridDim.x * blockDim.x)
+        out[id] = cvt<FT>(warp_sample(src, f, id, nx, ny, nz, volume, flow));
+}
+
 // Drop-in kernel_forwardDVF.
 static __global__ void __launch_bounds__(256) forward_dvf_kernel(float *mx, float *my, float *mz,
                                                                  Fields<float> f, int64_t n,
@@ -119,20 +132,22 @@ constexpr int WARP_ROWS = 2;
 // SART image pass, forward warp of the current volume into the view's phase:
 // dst[id] = warp(src)[id] stored in VT, plus the y-fastest copy
 // dstT[iy + ix*ny] of the result (x-fastest reading) for the projector.
-// blockDim (32, 8); block covers a 32 x (8 * WARP_ROWS) (x, y) tile of slice
+// blockDim (32, 8); block covers a 32 x (8 * WR) (x, y) tile of slice
 // blockIdx.z.
-template <typename SRC, typename FT, typename VT>
+// WR: rows of voxels per thread (the launch shape the driver's tuning may
+// choose; the same bits for every value).
+template <typename SRC, typename FT, typename VT, int WR = WARP_ROWS>
 static __global__ void __launch_bounds__(256) warp_fwd_kernel(VT *dst, VT *dstT, const SRC src,
                                                               Fields<FT> f, int nx, int ny,
                                                               int nz, float volume, float flow) {
-    constexpr int TH = 8 * WARP_ROWS;
+    constexpr int TH = 8 * WR;
     __shared__ float tile[TH][33];
     const int tx = threadIdx.x, ty = threadIdx.y;
     const int x0 = blockIdx.x * 32, y0 = blockIdx.y * TH, iz = blockIdx.z;
     const int64_t slice = (int64_t)iz * nx * ny;
     const int xm = x0 + tx;
 #pragma unroll
-    for (int k = 0; k < WARP_ROWS; k++) {
+    for (int k = 0; k < WR; k++) {
         const int ly = ty + 8 * k, ym = y0 + ly;
         float v = 0.0f;
         if (xm < nx && ym < ny) {
@@ -148,7 +163,7 @@ static __global__ void __launch_bounds__(256) warp_fwd_kernel(VT *dst, VT *dstT,
     // transposed store: runs of TH consecutive iy per ix
     const int t = ty * 32 + tx;
 #pragma unroll
-    for (int k = 0; k < WARP_ROWS; k++) {
+    for (int k = 0; k < WR; k++) {
         const int e = t + 256 * k, lx = e / TH, ly = e % TH;
         const int xmT = x0 + lx, ymT = y0 + ly;
         if (xmT < nx && ymT < ny) dstT[ymT + (int64_t)xmT * ny + slice] = cvt<VT>(tile[ly][lx]);
@@ -159,8 +174,8 @@ static __global__ void __launch_bounds__(256) warp_fwd_kernel(VT *dst, VT *dstT,
 // img[id] += lambda * warp(src)[id]  (AUMISART.cu:222-223).  With a surface,
 // the updated voxel is also written to the 3D array the next forward warp
 // samples through the texture unit.
-// blockDim (32, 8), 32 x (8 * WARP_ROWS) tiles of slice blockIdx.z.
-template <typename SRC, typename FT>
+// blockDim (32, 8), 32 x (8 * WR) tiles of slice blockIdx.z.
+template <typename SRC, typename FT, int WR = WARP_ROWS>
 static __global__ void __launch_bounds__(256) warp_back_add_kernel(
     float *img, cudaSurfaceObject_t img_surf, const SRC src, Fields<FT> f, int nx, int ny,
     int nz, float volume, float flow, float lambda) {
@@ -169,8 +184,8 @@ static __global__ void __launch_bounds__(256) warp_back_add_kernel(
     const int64_t slice = (int64_t)iz * nx * ny;
     if (xm >= nx) return;
 #pragma unroll
-    for (int k = 0; k < WARP_ROWS; k++) {
-        const int ym = blockIdx.y * (8 * WARP_ROWS) + ty + 8 * k;
+    for (int k = 0; k < WR; k++) {
+        const int ym = blockIdx.y * (8 * WR) + ty + 8 * k;
         if (ym >= ny) break;
         const int64_t id = xm + (int64_t)ym * nx + slice;
         int ix, iy;

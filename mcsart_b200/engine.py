@@ -191,6 +191,32 @@ class Context:
         self._call("mcsart_backprojection_adjoint", _ptr(d_img, "d_img", 4),
                    _ptr(d_proj, "d_proj", 4), angle, SO, SD, da, na, ai, db, nb, bi, nx, ny, nz)
 
+    @staticmethod
+    def _storage_of(t):
+        import torch
+        return {torch.float32: F32, torch.bfloat16: BF16, torch.float16: F16}[t.dtype]
+
+    def projection_ex(self, d_proj, d_img, angle, SO, SD, da, na, ai, db, nb, bi, nx, ny, nz, *,
+                      fp_sum=0, geom64=0):
+        """mcsart_projection_ex: d_img a float32, bfloat16 or float16 CUDA tensor."""
+        self._call("mcsart_projection_ex", _ptr(d_proj, "d_proj", 4), _ptr(d_img, "d_img"),
+                   self._storage_of(d_img), int(fp_sum), int(geom64), angle, SO, SD, da, na, ai,
+                   db, nb, bi, nx, ny, nz)
+
+    def backprojection_ex(self, d_img, d_proj, angle, SO, SD, da, na, ai, db, nb, bi, nx, ny, nz,
+                          *, geom64=0):
+        """mcsart_backprojection_ex (geom64 = 1: FP64 geometry)."""
+        self._call("mcsart_backprojection_ex", _ptr(d_img, "d_img", 4), _ptr(d_proj, "d_proj", 4),
+                   int(geom64), angle, SO, SD, da, na, ai, db, nb, bi, nx, ny, nz)
+
+    def deform_ex(self, d_img1, d_img, nx, ny, nz, volume, flow, fields, *, interp=INTERP_EXACT):
+        """mcsart_deform_ex: fields a (6, nz, ny, nx) CUDA tensor whose dtype (float32,
+        bfloat16, float16) is also the output's."""
+        if d_img1.dtype != fields.dtype:
+            raise ValueError("d_img1 and fields must have the same dtype")
+        self._call("mcsart_deform_ex", _ptr(d_img1, "d_img1"), _ptr(d_img, "d_img", 4), nx, ny,
+                   nz, volume, flow, _ptr(fields, "fields"), self._storage_of(fields), int(interp))
+
     def host_deform(self, d_img1, d_img, nx, ny, nz, volume, flow, alpha_x, alpha_y, alpha_z,
                     beta_x, beta_y, beta_z):
         """include/cu_deform.h:8"""
@@ -364,3 +390,36 @@ class Context:
         op = np.ascontiguousarray(op_iter, dtype=np.int32)
         self._call("mcsart_batch_run", arr, len(structs), int(n_iter), _hptr(op),
                    ctypes.byref(options) if options is not None else None)
+
+    def autotune(self, *, geo, n_views, lambda_, angles, volumes, flows, img, proj, fields=None,
+                 options=None) -> list:
+        """mcsart_autotune for one problem (same keyword arguments as
+        aumisart_device); returns the cached variant indices [fp1, fp3, bp, warp]."""
+        p, keep = self._problem(geo, n_views, lambda_, angles, volumes, flows, img, proj, fields,
+                                None, None, options)
+        self._call("mcsart_autotune", ctypes.byref(p),
+                   ctypes.byref(options) if options is not None else None)
+        storage = options.storage if options is not None else F32
+        return self.tuning_get(geo, storage)
+
+    def tuning_get(self, geo, storage=F32):
+        """Cached launch-shape variants [fp1, fp3, bp, warp] of a geometry, or None."""
+        p = Problem()
+        p.nx, p.ny, p.nz = int(geo["nx"]), int(geo["ny"]), int(geo["nz"])
+        p.na, p.nb = int(geo["na"]), int(geo["nb"])
+        p.SO, p.SD, p.da, p.db = geo["SO"], geo["SD"], geo["da"], geo["db"]
+        p.ai, p.bi = geo["ai"], geo["bi"]
+        out = (ctypes.c_int * 4)()
+        rc = self._L.mcsart_tuning_get(self._h, ctypes.byref(p), int(storage), out)
+        if rc < 0:
+            check(rc, "mcsart_tuning_get")
+        return list(out) if rc == 1 else None
+
+    def tuning_save(self, path) -> None:
+        self._call("mcsart_tuning_save", str(path).encode())
+
+    def tuning_load(self, path) -> int:
+        rc = self._L.mcsart_tuning_load(self._h, str(path).encode())
+        if rc < 0:
+            check(rc, "mcsart_tuning_load")
+        return rc

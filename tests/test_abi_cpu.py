@@ -64,6 +64,7 @@ def test_default_options(lib):
     o = Options()
     lib.mcsart_default_options(ctypes.byref(o))
     assert (o.storage, o.interp, o.use_graph, o.fp_sum, o.fp_groups) == (0, 0, 1, 0, 0)
+    assert (o.subset, o.dvf_inverse, o.geom64, o.autotune) == (1, 0, 0, 0)
 
 
 def test_python_context_raises_without_device():
