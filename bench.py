@@ -395,6 +395,78 @@ def run_kernel_case(args, ctx, torch, stream):
                               "y-fastest copy of the volume for x-driven rays)"}), flush=True)
 
 
+def run_batch_config(args, ctx, torch, stream, m, rank, world):
+    """--config c4: the 8 seeded uneven problems (96x96x64 .. 256x256x128,
+    detectors 192x128 .. 512x384, 120 .. 660 views) reconstructed together by
+    mcsart_batch_run, image passes in ordered subsets of 10 views.  One step =
+    one outer iteration (image pass + DVF-update pass) of every problem.
+    value = problem-iterations per second; beside it the same work as one
+    mcsart_aumisart_device call per problem after another, and the voxel-ray
+    updates per second of the batch."""
+    from mcsart_b200 import synthetic as S
+    cfgs = S.batch_configs()
+    op = np.array([1, 0], np.int32)
+    probs = []
+    for i, cfg in enumerate(cfgs):
+        p, proj, fields = build_problem(ctx, torch, cfg, seed=200 * (rank + 1) + i)
+        g = p.geo
+        probs.append(dict(geo=g, n_views=cfg.n_views, lambda_=p.cfg.lam, angles=p.angles,
+                          volumes=p.volumes, flows=p.flows, proj=proj,
+                          img=torch.zeros((g["nz"], g["ny"], g["nx"]), device="cuda"),
+                          fields=torch.stack(fields).contiguous()))
+        del fields
+    vox_rays = sum(q["geo"]["nx"] * q["geo"]["ny"] * q["geo"]["nz"] * q["n_views"] for q in probs)
+    flush = torch.empty(256 * 2**20 // 4, dtype=torch.float32, device="cuda")
+    out = {}
+    for label, storage in (("f32", m.F32), ("bf16", m.BF16)):
+        opt = m.default_options(subset=S.BATCH_SUBSET, storage=storage, autotune=1)
+        if storage == m.F32:
+            batch = probs
+        else:
+            batch = [dict(q, proj=q["proj"].to(torch.bfloat16),
+                          fields=q["fields"].to(torch.bfloat16)) for q in probs]
+
+        def batch_step():
+            ctx.batch_run(batch, n_iter=2, op_iter=op, options=opt)
+
+        def seq_step():
+            for q in batch:
+                ctx.aumisart_device(n_iter=2, op_iter=op, options=opt, **q)
+
+        res = {}
+        for name, fn in (("batch", batch_step), ("sequential", seq_step)):
+            for _ in range(args.warmup):
+                fn()
+            torch.cuda.synchronize()
+            ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                  for _ in range(args.steps)]
+            for e0, e1 in ev:
+                flush.fill_(1.0)
+                e0.record(stream)
+                fn()
+                e1.record(stream)
+            torch.cuda.synchronize()
+            t = max_over_ranks(sum(a.elapsed_time(b) for a, b in ev) / 1000.0)
+            res[name] = len(probs) * args.steps / t * world
+        out[label] = res
+        del batch
+    line = {"metric": "McSART iterations/s (all problems)", "value": out["f32"]["batch"],
+            "unit": "problem-iterations/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000.0 * len(probs) / out["f32"]["batch"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": "c4: 8 uneven motion-compensated problems, one outer "
+                                   "iteration each per step, ordered subsets of 10 views",
+                       "problems": [c.name for c in cfgs],
+                       "l2": "flushed before every timed step (256 MiB write)"},
+            "voxel_ray_updates_per_s": out["f32"]["batch"] / len(probs) * vox_rays,
+            "sequential_f32": out["f32"]["sequential"], "batch_bf16": out["bf16"]["batch"],
+            "sequential_bf16": out["bf16"]["sequential"],
+            "tuned_shapes": {c.name: ctx.tuning_get(q["geo"]) for c, q in zip(cfgs, probs)}}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -420,6 +492,12 @@ def main():
     if args.kernel_case:
         if rank == 0:
             run_kernel_case(args, ctx, torch, stream)
+        ctx.close()
+        if dist_on:
+            dist.destroy_process_group()
+        return
+    if args.config == "c4":
+        run_batch_config(args, ctx, torch, stream, m, rank, world)
         ctx.close()
         if dist_on:
             dist.destroy_process_group()

@@ -6,6 +6,10 @@ The workloads follow the benchmark configurations of the McSART engine:
   config 2: motion-compensated, 128x128x96 at 2 mm, 256x192 at 1.2 mm, 360 views,
             10 outer iterations of SART + DVF update
   config 3: motion-compensated, 256x256x160 at 1 mm, 512x384 at 0.776 mm, 660 views
+  config 4: 8 independent motion-compensated problems of seeded uneven sizes
+            (volumes 96x96x64 to 256x256x128 at 1-2 mm, detectors 192x128 to
+            512x384, 120-660 views each), reconstructed together in ordered
+            subsets of 10 views (``batch_configs``)
   config 5: 512x512x256 at 0.5 mm, 1024x768 at 0.388 mm, 1320 views
 
 Phantom: 10 ellipsoids with centres uniform in a 50 mm ball, semi-axes U[5, 40] mm,
@@ -55,6 +59,40 @@ CONFIGS = {
     "c5": Config("clinical McSART 512x512x256, 1320 views", 512, 512, 256, 0.5, 1024, 768, 0.388,
                  1320, 10, True, True, si_mm=15.0, aplr_mm=4.5),
 }
+
+
+# The uneven batch: sizes drawn from these sets with a seeded generator.
+BATCH_SLICES = (96, 128, 160, 192, 224, 256)
+BATCH_DEPTHS = (64, 96, 128)
+BATCH_VOXEL_MM = (1.0, 1.5, 2.0)
+BATCH_DETECTORS = ((192, 128), (256, 192), (384, 288), (512, 384))
+BATCH_SUBSET = 10
+
+
+def batch_configs(n: int = 8, seed: int = 0) -> list[Config]:
+    """The uneven batch of config 4: n motion-compensated problems of seeded
+    sizes.  The first two are the extremes (96x96x64 with a 192x128 detector
+    and 120 views; 256x256x128 with 512x384 and 660 views), the others drawn
+    from the size sets above; views are multiples of the subset size 10 in
+    [120, 660].  The detector pitch makes the detector cover the volume's
+    width magnified by SDD/SAD = 1.5 with a 10 % margin."""
+    rng = np.random.default_rng(seed + 4)
+    out = []
+    for i in range(n):
+        if i == 0:
+            nxy, nz, vox, (na, nb), nv = 96, 64, 2.0, BATCH_DETECTORS[0], 120
+        elif i == 1:
+            nxy, nz, vox, (na, nb), nv = 256, 128, 1.0, BATCH_DETECTORS[-1], 660
+        else:
+            nxy = int(rng.choice(BATCH_SLICES))
+            nz = int(rng.choice(BATCH_DEPTHS))
+            vox = float(rng.choice(BATCH_VOXEL_MM))
+            na, nb = BATCH_DETECTORS[int(rng.integers(len(BATCH_DETECTORS)))]
+            nv = int(rng.integers(12, 67)) * BATCH_SUBSET
+        pitch = round(1.5 * 1.1 * nxy * vox / na, 3)
+        out.append(Config(f"batch problem {i}: {nxy}x{nxy}x{nz} at {vox} mm, {na}x{nb}, {nv} views",
+                          nxy, nxy, nz, vox, na, nb, pitch, nv, 10, True, True))
+    return out
 
 
 def geometry(cfg: Config) -> dict:
