@@ -55,6 +55,9 @@ def parse():
     ap.add_argument("--profile-steps", type=int, default=0,
                     help="only run this many untimed steps inside the NVTX range "
                          "'mcsart_step' (for a profiler's launch list) and exit")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="run the driver with its built-in launch shapes instead of tuning "
+                         "them for the workload in the warm-up (mcsart_autotune)")
     ap.add_argument("--kernel-case", default="", choices=["", "fp", "bp", "warp"],
                     help="only time single calls of one kernel at the workload's size "
                          "(projector, backprojector or warp through the C ABI, CUDA events, "
@@ -542,7 +545,9 @@ def main():
         total = max_over_ranks(sum(a.elapsed_time(b) for a, b in ev) / 1000.0)
         return total, launches
 
-    drop_in = m.default_options()  # FP32, texture-model warp, reference summation order
+    # FP32, texture-model warp, reference summation order; launch shapes tuned
+    # for the workload on the first (warm-up) run, which changes no result bit
+    drop_in = m.default_options(autotune=0 if args.no_autotune else 1)
     if args.profile_steps:
         for _ in range(args.profile_steps):
             torch.cuda.nvtx.range_push("mcsart_step")
@@ -630,7 +635,7 @@ def main():
                          ("subsets_of_8_f32", dict(subset=8)),
                          ("subsets_of_8_bf16", dict(subset=8, storage=m.BF16,
                                                     interp=m.INTERP_EXACT))):
-            o = m.default_options(**kw)
+            o = m.default_options(autotune=drop_in.autotune, **kw)
             if o.storage == m.F32:
                 pr, Ft = proj, (F0.clone() if F0 is not None else None)
             else:
@@ -700,6 +705,8 @@ def main():
                 "config": config_dict(p, args), "voxel_ray_updates_per_s": vox_ray,
                 "e2e": e2e, "gpu_launches": int(launches), "roofline": roofline,
                 "cpu_baseline": cpu, "clocks": clk, "kernel_ms_per_step": kernel_ms,
+                "launch_shapes": {"autotuned": bool(drop_in.autotune),
+                                  "variants_fp1_fp3_bp_warp": ctx.tuning_get(g)},
                 "extras": extras}
         print(json.dumps(line), flush=True)
     ctx.close()

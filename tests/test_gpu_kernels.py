@@ -193,22 +193,22 @@ def test_elementwise_match_reference(ctx, torch_cuda, ref):
     np.testing.assert_array_equal(out, ref.add(a, b, -0.7))
     for ind in (1, 2, 3):
         out = run(lambda x, y, z: ctx.host_add2(x, y, nx, ny, nz, z, 0.6, ind), a, b, c)[0]
-        np.testing.assert_allclose(out, ref.add2(a, b, c, 0.6, ind), rtol=0, atol=1e-6)
+        np.testing.assert_array_equal(out, ref.add2(a, b, c, 0.6, ind))
         out = run(lambda x, z: ctx.host_multiple(x, nx, ny, nz, z, 1.4, ind), a, c)[0]
-        np.testing.assert_allclose(out, ref.multiple(a, c, 1.4, ind), rtol=0, atol=1e-6)
+        np.testing.assert_array_equal(out, ref.multiple(a, c, 1.4, ind))
         out = run(lambda x, y: ctx.host_diff(x, y, nx, ny, nz, ind), np.zeros_like(a), b)[0]
         np.testing.assert_array_equal(out, ref.diff(b, ind))
     out = run(lambda x: ctx.host_initial(x, nx, ny, nz, 2.5), a)[0]
     np.testing.assert_array_equal(out, ref.initial(shape, 2.5))
     out = run(lambda x, z: ctx.host_initial2(x, nx, ny, nz, z, -0.4, 1.9), a, c)[0]
-    np.testing.assert_allclose(out, ref.initial2(c, -0.4, 1.9), rtol=0, atol=1e-6)
+    np.testing.assert_array_equal(out, ref.initial2(c, -0.4, 1.9))
     out = run(lambda x, y: ctx.host_division(x, y, nx, ny, nz), a, b)[0]
     np.testing.assert_array_equal(out, ref.division(a, b))
     assert np.all(out[0, 0, :5] == 0.0)
     outs = run(lambda *t: ctx.host_update_udvf(*t[:6], t[6], t[7], 0.9, -0.5, nx, ny, nz),
                *F, b, c)
     for x, y in zip(outs[:6], ref.update_udvf(F, b, c, 0.9, -0.5)):
-        np.testing.assert_allclose(x, y, rtol=1e-6, atol=1e-6)
+        np.testing.assert_array_equal(x, y)
 
 
 def test_projection_residual_on_projection_shape(ctx, torch_cuda, ref):
