@@ -37,6 +37,25 @@ bool view_has_xdrive(float angle, const Geom &g) {
     return false;
 }
 
+// Which volume copies a view's projector reads: x-driven rays read the
+// y-fastest copy, y-driven rays the x-fastest one.  Evaluated with the float
+// arithmetic of the kernel's ray set-up and a margin for the last bit of the
+// host's and the device's sine and cosine, so a column near the switch
+// counts for both.
+void view_drive_axes(float angle, const Geom &g, bool *any_x, bool *any_y) {
+    const float cphi = cosf(angle), sphi = sinf(angle);
+    const float x1 = -g.SO * cphi, y1 = -g.SO * sphi;
+    const float x20 = g.SD - g.SO;
+    *any_x = *any_y = false;
+    for (int ia = 0; ia < g.na; ia++) {
+        const float y20 = (ia + g.ai) * g.da;
+        const float x21 = (x20 * cphi - y20 * sphi) - x1;
+        const float y21 = (x20 * sphi + y20 * cphi) - y1;
+        if (fabsf(x21) >= 0.999f * fabsf(y21)) *any_x = true;
+        if (fabsf(y21) >= 0.999f * fabsf(x21)) *any_y = true;
+    }
+}
+
 template <int K>
 int launch_fp_plain(mcsart_ctx *ctx, float *d_proj, const float *d_img, const float *d_imgT,
                     float angle, const float *d_angles, int n_views, const Geom &g) {

@@ -185,7 +185,9 @@ __device__ __forceinline__ void load_tile_T(float (*tile)[33], const T *src, int
 // Motion pass, AUMISART.cu:252-258 and :267 fused: for the current view
 //   img0 = sum over the six (field, gradient) pairs of F[t]*w*d img
 //   ones = (dx + dy + dz img) * (-vd + -fd)
-// each written x-fastest and as a y-fastest copy for the projector.
+// each written x-fastest (img0, ones) and as a y-fastest copy (img0T,
+// onesT) for the projector; either pair may be nullptr when the view's
+// projector reads only the other.
 template <typename FT, typename VT>
 static __global__ void __launch_bounds__(256) motion_prep_kernel(VT *img0, VT *img0T, VT *ones,
                                                           VT *onesT, const float *img,
@@ -223,12 +225,15 @@ static __global__ void __launch_bounds__(256) motion_prep_kernel(VT *img0, VT *i
             a = __fmaf_rn(ft[4][tx][ly] * fd, dfy, a);
             a = __fmaf_rn(ft[5][tx][ly] * fd, dfz, a);
             b = (dfx + dfy + dfz) * s_ones;  // cu_initial.cu:48
-            img0[id] = cvt<VT>(a);
-            ones[id] = cvt<VT>(b);
+            if (img0) {
+                img0[id] = cvt<VT>(a);
+                ones[id] = cvt<VT>(b);
+            }
         }
         o0[ly][tx] = a;
         o1[ly][tx] = b;
     }
+    if (img0T == nullptr) return;  // uniform over the block
     __syncthreads();
 #pragma unroll
     for (int k = 0; k < 4; k++) {
@@ -349,12 +354,15 @@ static __global__ void __launch_bounds__(256) field_update_prep_kernel(
             a = __fmaf_rn(ft[4][tx][ly] * fd, dfy, a);
             a = __fmaf_rn(ft[5][tx][ly] * fd, dfz, a);
             b = (dfx + dfy + dfz) * s_ones;  // cu_initial.cu:48
-            img0[id] = cvt<VT>(a);
-            ones[id] = cvt<VT>(b);
+            if (img0) {
+                img0[id] = cvt<VT>(a);
+                ones[id] = cvt<VT>(b);
+            }
         }
         o0[ly][tx] = a;
         o1[ly][tx] = b;
     }
+    if (img0T == nullptr) return;  // uniform over the block
     __syncthreads();
 #pragma unroll
     for (int k = 0; k < 4; k++) {

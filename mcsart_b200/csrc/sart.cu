@@ -75,6 +75,7 @@ template <typename ST, int INTERP, int SUM> struct Runner {
     int inv_iters = 0;  // fixed-point steps of the true DVF inverse (0: negated amplitudes)
     int cols_view = -1;  // view whose backprojector column data the last projector wrote
     std::vector<int> views_img, views_mot;
+    std::vector<char> reads_std, reads_tr;  // per view: the copies its projector reads
     Tuning tune;  // launch shapes (variant indices; -1 = built-in choice)
 
     Runner(mcsart_ctx *c, const Problem &p, const mcsart_options &o)
@@ -93,7 +94,19 @@ template <typename ST, int INTERP, int SUM> struct Runner {
         for (int v = 0; v < P.n_views; v++) views_img.push_back(v);
         const int step = P.motion_model ? 1 : 10;  // AUMISART.cu:242 vs :72
         for (int v = 1; v < P.n_views; v += step) views_mot.push_back(v);
+        reads_std.resize(P.n_views);
+        reads_tr.resize(P.n_views);
+        for (int v = 0; v < P.n_views; v++) {
+            bool ax, ay;
+            view_drive_axes(P.angles[v], P.g, &ax, &ay);
+            reads_tr[v] = ax;
+            reads_std[v] = ay;
+        }
     }
+
+    // A per-view copy of a volume the projector of view v reads, else nullptr.
+    ST *std_or_null(int v, const DevBuf &b) const { return reads_std[v] ? b.as<ST>() : nullptr; }
+    ST *tr_or_null(int v, const DevBuf &b) const { return reads_tr[v] ? b.as<ST>() : nullptr; }
 
     Fields<ST> fields() const {
         const ST *f = (const ST *)P.fields;
@@ -308,28 +321,30 @@ template <typename ST, int INTERP, int SUM> struct Runner {
         return dim3(div_up(P.g.nx, 32), div_up(P.g.ny, 8 * WR), P.g.nz);
     }
 
-    // The image pass's forward warp of the volume into a view's phase, in the
-    // tuned launch shape (voxel rows per thread).
-    template <int WR> int warp_fwd_shape(bool hw, float volume, float flow) {
+    // The image pass's forward warp of the volume into view v's phase, in
+    // the tuned launch shape (voxel rows per thread), writing only the
+    // copies view v's projector reads.
+    template <int WR> int warp_fwd_shape(int v, bool hw, float volume, float flow) {
         const Geom &g = P.g;
         const Fields<ST> f = fields();
+        ST *d = reads_std[v] ? S.img1.as<ST>() : nullptr;
+        ST *dT = reads_tr[v] ? S.img1T.as<ST>() : nullptr;
         ctx->label = "warp_fwd";
         if (hw) {
             MC_LAUNCH(ctx, (warp_fwd_kernel<SrcTex, ST, ST, WR>), warp_grid<WR>(), dim3(32, 8), 0,
-                      S.img1.as<ST>(), S.img1T.as<ST>(), SrcTex{S.tv_img.tex}, f, g.nx, g.ny,
-                      g.nz, volume, flow);
+                      d, dT, SrcTex{S.tv_img.tex}, f, g.nx, g.ny, g.nz, volume, flow);
         } else {
             MC_LAUNCH(ctx, (warp_fwd_kernel<SrcLinear<float>, ST, ST, WR>), warp_grid<WR>(),
-                      dim3(32, 8), 0, S.img1.as<ST>(), S.img1T.as<ST>(), SrcLinear<float>{P.img},
-                      f, g.nx, g.ny, g.nz, volume, flow);
+                      dim3(32, 8), 0, d, dT, SrcLinear<float>{P.img}, f, g.nx, g.ny, g.nz, volume,
+                      flow);
         }
         return MCSART_OK;
     }
-    int warp_fwd(bool hw, float volume, float flow) {
+    int warp_fwd(int v, bool hw, float volume, float flow) {
         switch (tune.warp) {
-            case 1: return warp_fwd_shape<1>(hw, volume, flow);
-            case 2: return warp_fwd_shape<4>(hw, volume, flow);
-            default: return warp_fwd_shape<WARP_ROWS>(hw, volume, flow);
+            case 1: return warp_fwd_shape<1>(v, hw, volume, flow);
+            case 2: return warp_fwd_shape<4>(v, hw, volume, flow);
+            default: return warp_fwd_shape<WARP_ROWS>(v, hw, volume, flow);
         }
     }
     // The backward warp of a view's correction and the update, tuned shape.
@@ -486,7 +501,7 @@ template <typename ST, int INTERP, int SUM> struct Runner {
             const int v = views_img[k];
             const float volume = P.volumes[v] - P.volumes[0];   // :193
             const float flow = P.flows[v] - P.flows[0];
-            MC_TRY(warp_fwd(hw, volume, flow));
+            MC_TRY(warp_fwd(v, hw, volume, flow));
             MC_TRY((launch_fp<1, true, ST>(vol, v, k, FP_IMAGE)));
             if (hw)
                 MC_TRY(launch_bp(v, BP_DIV, nullptr, nullptr, S.tv_ratio.surf));
@@ -529,8 +544,9 @@ template <typename ST, int INTERP, int SUM> struct Runner {
             if (!fuse || k == 0) {
                 ctx->label = "motion_prep";
                 MC_LAUNCH(ctx, (motion_prep_kernel<ST, ST>), tile_grid(), dim3(32, 8), 0,
-                          S.img0.as<ST>(), S.img0T.as<ST>(), S.ones.as<ST>(), S.onesT.as<ST>(),
-                          (const float *)P.img, f, g.nx, g.ny, g.nz, vd, fd);
+                          std_or_null(v, S.img0), tr_or_null(v, S.img0T), std_or_null(v, S.ones),
+                          tr_or_null(v, S.onesT), (const float *)P.img, f, g.nx, g.ny, g.nz, vd,
+                          fd);
             }
             MC_TRY((launch_fp<3, false, ST>(vol, v, k, FP_MOTION)));
             MC_TRY(launch_bp(v, BP_DIV, S.ratio.as<float>(), nullptr));
@@ -544,8 +560,8 @@ template <typename ST, int INTERP, int SUM> struct Runner {
                 MC_LAUNCH(ctx, (field_update_prep_kernel<ST, ST>), tile_grid(), dim3(32, 8), 0,
                           fw, fw + V, fw + 2 * V, fw + 3 * V, fw + 4 * V, fw + 5 * V,
                           (const float *)S.ratio.as<float>(), (const float *)P.img, g.nx, g.ny,
-                          g.nz, nvd, nfd, S.img0.as<ST>(), S.img0T.as<ST>(), S.ones.as<ST>(),
-                          S.onesT.as<ST>(), vdn, fdn);
+                          g.nz, nvd, nfd, std_or_null(vn, S.img0), tr_or_null(vn, S.img0T),
+                          std_or_null(vn, S.ones), tr_or_null(vn, S.onesT), vdn, fdn);
             } else {
                 ctx->label = "field_update";
                 MC_LAUNCH(ctx, (field_update_kernel<ST>), tile_grid(), dim3(32, 8), 0, fw, fw + V,

@@ -43,6 +43,11 @@ struct Problem {
     float *resid;                           // device FP32 or nullptr
 };
 
+// Which volume copies the projector reads for a view (abi_kernels.cu):
+// any_x: some rays are x-driven (the y-fastest copy), any_y: some are
+// y-driven (the x-fastest volume).
+void view_drive_axes(float angle, const Geom &g, bool *any_x, bool *any_y);
+
 // Runs n_iter passes of host_AUMISART's loop (sart.cu).
 int run_driver(mcsart_ctx *ctx, const Problem &P, int n_iter, const int *op_iter, float *norm_out,
                const mcsart_options &opt);

@@ -132,6 +132,8 @@ constexpr int WARP_ROWS = 2;
 // SART image pass, forward warp of the current volume into the view's phase:
 // dst[id] = warp(src)[id] stored in VT, plus the y-fastest copy
 // dstT[iy + ix*ny] of the result (x-fastest reading) for the projector.
+// Either output may be nullptr when the view's projector reads only the
+// other (all its rays driven along y, or all along x).
 // blockDim (32, 8); block covers a 32 x (8 * WR) (x, y) tile of slice
 // blockIdx.z.
 // WR: rows of voxels per thread (the launch shape the driver's tuning may
@@ -155,10 +157,11 @@ static __global__ void __launch_bounds__(256) warp_fwd_kernel(VT *dst, VT *dstT,
             int ix, iy;
             warp_coords(xm, ym, nx, ny, ix, iy);
             v = warp_sample_at(src, f, id, ix, iy, iz, nx, ny, nz, volume, flow);
-            dst[id] = cvt<VT>(v);
+            if (dst) dst[id] = cvt<VT>(v);
         }
         tile[ly][tx] = v;
     }
+    if (dstT == nullptr) return;  // uniform over the block
     __syncthreads();
     // transposed store: runs of TH consecutive iy per ix
     const int t = ty * 32 + tx;
