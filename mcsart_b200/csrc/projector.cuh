@@ -462,9 +462,11 @@ struct __align__(16) SlabC {
     float a, b;  // SlabU's
     float dc;
     int U1, U2;
-    int flags;   // SC_U0 | SC_U1 | SC_NARROW (U2 - U1 <= 1)
+    int flags;   // SC_U0 | SC_U1 | SC_NARROW (U2 - U1 <= 1) | SC_UANY
 };
-constexpr int SC_U0 = 1, SC_U1 = 2, SC_NARROW = 4;
+// SC_UANY: the reference's in-plane loop over max(0, U1) .. min(nu-1, U2) is
+// not empty (:80-81 / :133-134)
+constexpr int SC_U0 = 1, SC_U1 = 2, SC_NARROW = 4, SC_UANY = 8;
 
 __device__ __forceinline__ SlabC slab_c(const RayGeom &r, int d, int su, int sd) {
     const SlabU e = slab_u(r, d);
@@ -477,7 +479,8 @@ __device__ __forceinline__ SlabC slab_c(const RayGeom &r, int d, int su, int sd)
     const int U1 = e.U1, U2 = e.U2;
     const bool u0 = U1 >= 0 && U1 <= r.nu - 1;
     const bool u1 = U1 + 1 <= U2 && U1 + 1 >= 0 && U1 + 1 <= r.nu - 1;
-    c.flags = (u0 ? SC_U0 : 0) | (u1 ? SC_U1 : 0) | (U2 - U1 <= 1 ? SC_NARROW : 0);
+    c.flags = (u0 ? SC_U0 : 0) | (u1 ? SC_U1 : 0) | (U2 - U1 <= 1 ? SC_NARROW : 0) |
+              (U2 >= 0 && U1 <= r.nu - 1 ? SC_UANY : 0);
     const int cu0 = min(max(U1, 0), r.nu - 1), cu1 = min(max(U1 + 1, 0), r.nu - 1);
     c.r0 = cu0 * su + d * sd;
     c.r1 = cu1 * su + d * sd;
@@ -577,6 +580,53 @@ __device__ __forceinline__ RayAxial ray_axial(const RayGeom &r, float z_half) {
     const bool off1 = fminf(e1a, e1b) > tiny || fmaxf(e1a, e1b) < -tiny;
     a.exact = a.zsafe && one_sign && dz_min >= 0x1p-19f && off0 && off1;
     return a;
+}
+
+// The slabs d of a ray whose axial footprint can meet the volume: a superset
+// of {d : max(cz0, cz1) >= 0 and min(cz0, cz1) < nz}, outside which the
+// reference's axial loop over max(0, Z1) .. min(nz-1, Z2) is empty
+// (:80-82 / :133-135) and the slab adds nothing.  Worked from the exact lines
+// c_k(dc) = rz_k * dc + nz/2 of the ray's own (float) constants with a
+// tolerance of 1/64 voxel, far above the difference of their float
+// evaluation (a few ulp of values below 2^20); each condition's set of dc is
+// a union of half-lines whose hull is taken, and the intersection of the
+// hulls is mapped to slab indices with one slab of margin on either side.
+// Returns lo > hi when no slab can contribute.
+__device__ __forceinline__ void ray_zrange(const RayGeom &r, float z_half, int nz, int &lo,
+                                           int &hi) {
+    const double tol = 1.0 / 64.0, zh = z_half, rz[2] = {r.rz0, r.rz1};
+    const double inf = 1e300;
+    // hull of F1 = U_k {rz_k dc >= -tol - zh}: [lo1, hi1]
+    double lo1 = inf, hi1 = -inf;
+    // hull of F2 = U_k {rz_k dc < nz + tol - zh}: [lo2, hi2]
+    double lo2 = inf, hi2 = -inf;
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+        const double a = rz[k];
+        const double t1 = (-tol - zh) / a, t2 = ((double)nz + tol - zh) / a;
+        if (a > 0.0) {
+            lo1 = fmin(lo1, t1); hi1 = inf;    // [t1, inf)
+            lo2 = -inf; hi2 = fmax(hi2, t2);   // (-inf, t2)
+        } else if (a < 0.0) {
+            lo1 = -inf; hi1 = fmax(hi1, t1);   // (-inf, t1]
+            lo2 = fmin(lo2, t2); hi2 = inf;    // (t2, inf)
+        } else {  // constant zh: inside [0, nz)
+            lo1 = -inf; hi1 = inf;
+            lo2 = -inf; hi2 = inf;
+        }
+    }
+    const double dlo = fmax(lo1, lo2), dhi = fmin(hi1, hi2);
+    // slab d has dc = d + 0.5 - d_half - src_d (up to the rounding of
+    // those floats)
+    const double off = (double)r.d_half + (double)r.src_d - 0.5;
+    const double a = fmax(dlo + off, -2.0), b = fmin(dhi + off, (double)r.nd + 1.0);
+    if (!(a <= b)) {  // also NaN
+        lo = 1;
+        hi = 0;
+        return;
+    }
+    lo = max(0, (int)floor(a) - 1);
+    hi = min(r.nd - 1, (int)ceil(b) + 1);
 }
 
 // One slab of one ray, any footprint: the 2x2 window with predication or the
@@ -711,26 +761,27 @@ __device__ __forceinline__ void fp_group_sum(const RayGeom &r, const Geom &g,
     }
 }
 
-// Slabs d0 .. d0 + dn - 1 of a ray from the shared table.  Groups of G
-// slabs: the windows and loads of a whole group are issued together
-// before its terms enter the sums in the reference's order, so that a warp
-// waits for memory once per group instead of per slab.  A group whose
-// footprints are not all 2x2 windows takes the general per-slab path.
+// Slabs d0 + j0 .. d0 + jend - 1 of a ray from the shared table (j0 is the
+// same for the whole warp).  Groups of G slabs: the windows and loads of a
+// whole group are issued together before its terms enter the sums in the
+// reference's order, so that a warp waits for memory once per group instead
+// of per slab.  A group whose footprints are not all 2x2 windows takes the
+// general per-slab path.
 template <int K, int G, bool ONES, typename VT, bool CHECK>
 __device__ __forceinline__ void fp_chunk(const RayGeom &r, const Geom &g,
-                                         const SlabC (*sm_c)[FPC_COLS], int col, int dn, int d0,
-                                         const VT *const *base, int su, int sd, int sz, float z_half,
-                                         bool zsafe, float *acc, float &accw) {
-    const int ng = dn / G;
-    for (int i = 0; i < ng; i++) {
+                                         const SlabC (*sm_c)[FPC_COLS], int col, int j0, int jend,
+                                         int d0, const VT *const *base, int su, int sd, int sz,
+                                         float z_half, bool zsafe, float *acc, float &accw) {
+    int j = j0;
+    for (; j + G <= jend; j += G) {
         SlabZ w[G];
         float v[G][K][4];
-        const bool fast = fp_group_load<K, G, CHECK>(r, g, sm_c, col, i * G, sz, base, z_half,
+        const bool fast = fp_group_load<K, G, CHECK>(r, g, sm_c, col, j, sz, base, z_half,
                                                   zsafe, w, v);
-        fp_group_sum<K, G, ONES, VT, CHECK>(r, g, sm_c, col, i * G, d0, base, su, sd, sz,
+        fp_group_sum<K, G, ONES, VT, CHECK>(r, g, sm_c, col, j, d0, base, su, sd, sz,
                                          z_half, zsafe, fast, w, v, acc, accw);
     }
-    for (int j = ng * G; j < dn; j++)
+    for (; j < jend; j++)
         fp_slab<K, ONES, VT, CHECK>(r, g, sm_c[j][col], d0 + j, base, su, sd, sz, z_half, zsafe, acc,
                                     accw);
 }
@@ -765,6 +816,8 @@ template <int K, bool ONES, typename VT, typename MT = VT, bool MULTI = false,
 __global__ void __launch_bounds__(FPC_THREADS, MINB) fp_ref_kernel(const FPArgs<VT, K, MT> p) {
     __shared__ SlabC sm_c[FPC_CHUNK][FPC_COLS];
     __shared__ double2 sm_norm[FPC_THREADS / 32];
+    __shared__ int sm_wr[FPC_THREADS / 32][2];  // each warp's slab range
+    __shared__ int sm_ur[2];                    // the chunk's in-plane slab range
     const Geom &g = p.g;
     const int t = threadIdx.x, col = t % FPC_COLS, row = t / FPC_COLS;
     const int ia = blockIdx.x * FPC_COLS + col, ib = blockIdx.y * FPC_ROWS + row;
@@ -803,8 +856,30 @@ __global__ void __launch_bounds__(FPC_THREADS, MINB) fp_ref_kernel(const FPArgs<
     // range checks (warp-uniform, so neither form diverges)
     const RayAxial ax = ray_axial(r, z_half);
     const bool warp_exact = __all_sync(0xffffffffu, !active || ax.exact);
-    const int nd_max = max(g.nx, g.ny);
-    for (int d0 = 0; d0 < nd_max; d0 += FPC_CHUNK) {
+    // Slabs that can add to some ray of the warp: the union of the rays'
+    // axial ranges (ray_zrange); the block visits the union of its warps'.
+    // Outside them, and outside the slabs where some column of the block
+    // meets the volume in-plane (SC_UANY), the reference's loops are empty.
+    int zlo = 1, zhi = 0;
+    if (active) ray_zrange(r, z_half, g.nz, zlo, zhi);
+    if (zlo > zhi) {
+        zlo = INT_MAX;
+        zhi = INT_MIN;
+    }
+    const int wlo = __reduce_min_sync(0xffffffffu, zlo), whi = __reduce_max_sync(0xffffffffu, zhi);
+    if ((t & 31) == 0) {
+        sm_wr[t >> 5][0] = wlo;
+        sm_wr[t >> 5][1] = whi;
+    }
+    __syncthreads();
+    int blo = INT_MAX, bhi = INT_MIN;
+#pragma unroll
+    for (int w = 0; w < FPC_THREADS / 32; w++) {
+        blo = min(blo, sm_wr[w][0]);
+        bhi = max(bhi, sm_wr[w][1]);
+    }
+    const int first = blo <= bhi ? blo - blo % FPC_CHUNK : 0;
+    for (int d0 = first; d0 <= bhi; d0 += FPC_CHUNK) {
         for (int j = row; j < FPC_CHUNK; j += FPC_ROWS) {
             const int d = d0 + j;
             SlabC e;
@@ -814,13 +889,37 @@ __global__ void __launch_bounds__(FPC_THREADS, MINB) fp_ref_kernel(const FPArgs<
             sm_c[j][col] = e;
         }
         __syncthreads();
-        const int dn = active ? min(FPC_CHUNK, r.nd - d0) : 0;
+        if (t < 32) {  // the chunk's slabs where some column meets the volume in-plane
+            unsigned m[FPC_CHUNK / 32];
+#pragma unroll
+            for (int h = 0; h < FPC_CHUNK / 32; h++) {
+                bool any = false;
+#pragma unroll
+                for (int c = 0; c < FPC_COLS; c++) any |= (sm_c[h * 32 + t][c].flags & SC_UANY) != 0;
+                m[h] = __ballot_sync(0xffffffffu, any);
+            }
+            if (t == 0) {
+                int lo = FPC_CHUNK, hi = -1;
+#pragma unroll
+                for (int h = FPC_CHUNK / 32 - 1; h >= 0; h--)
+                    if (m[h]) lo = h * 32 + __ffs(m[h]) - 1;
+#pragma unroll
+                for (int h = 0; h < FPC_CHUNK / 32; h++)
+                    if (m[h]) hi = h * 32 + 31 - __clz(m[h]);
+                sm_ur[0] = lo;
+                sm_ur[1] = hi;
+            }
+        }
+        __syncthreads();
+        // (an empty warp range is wlo = INT_MAX > whi = INT_MIN)
+        const int j0 = wlo <= whi ? max(sm_ur[0], wlo - d0) : 0;
+        const int jend = (active && wlo <= whi) ? min(min(sm_ur[1], whi - d0) + 1, r.nd - d0) : 0;
         if (warp_exact)
-            fp_chunk<K, G, ONES, VT, false>(r, g, sm_c, col, dn, d0, base, su, sd, sz, z_half, ax.zsafe,
-                                         acc, accw);
+            fp_chunk<K, G, ONES, VT, false>(r, g, sm_c, col, max(j0, 0), jend, d0, base, su, sd,
+                                         sz, z_half, ax.zsafe, acc, accw);
         else
-            fp_chunk<K, G, ONES, VT, true>(r, g, sm_c, col, dn, d0, base, su, sd, sz, z_half, ax.zsafe,
-                                        acc, accw);
+            fp_chunk<K, G, ONES, VT, true>(r, g, sm_c, col, max(j0, 0), jend, d0, base, su, sd, sz,
+                                        z_half, ax.zsafe, acc, accw);
         __syncthreads();
     }
 
