@@ -791,6 +791,15 @@ __device__ __forceinline__ void fp_chunk(const RayGeom &r, const Geom &g,
 // MULTI = true: several views per launch (ordered subsets, kernel-level
 // multi-view projection), view = blockIdx.z with the per-view offsets of
 // FPArgs; false: one view per launch without them.
+// Row block i of n in dispatch order, from the middle of the detector
+// outwards (m, m+1, m-1, m+2, ...): central rays cross the whole volume,
+// outer ones fewer slabs (ray_zrange), so the longest blocks start first and
+// the short ones fill the last wave.
+__device__ __forceinline__ int middle_out(int i, int n) {
+    const int m = (n - 1) / 2;
+    return (i & 1) ? m + (i + 1) / 2 : m - i / 2;
+}
+
 // Whether a launch of bx x by projector blocks is resident at once with
 // FPC_MIN_BLOCKS blocks per SM (so that the larger register budget of deeper
 // slab groups costs no occupancy).
@@ -820,7 +829,8 @@ __global__ void __launch_bounds__(FPC_THREADS, MINB) fp_ref_kernel(const FPArgs<
     __shared__ int sm_ur[2];                    // the chunk's in-plane slab range
     const Geom &g = p.g;
     const int t = threadIdx.x, col = t % FPC_COLS, row = t / FPC_COLS;
-    const int ia = blockIdx.x * FPC_COLS + col, ib = blockIdx.y * FPC_ROWS + row;
+    const int by = middle_out(blockIdx.y, gridDim.y);  // this block's row block
+    const int ia = blockIdx.x * FPC_COLS + col, ib = by * FPC_ROWS + row;
     const bool col_ok = ia < g.na;
     const bool active = col_ok && ib < g.nb;
     const float angle = p.angles ? p.angles[blockIdx.z] : p.angle;
@@ -978,7 +988,7 @@ __global__ void __launch_bounds__(FPC_THREADS, MINB) fp_ref_kernel(const FPArgs<
             tr += sm_norm[w].y;
         }
         const int64_t vblk = MULTI ? (int64_t)blockIdx.z * gridDim.x * gridDim.y : 0;
-        p.norm_part[vblk + blockIdx.y * gridDim.x + blockIdx.x] = make_double2(tb, tr);
+        p.norm_part[vblk + by * gridDim.x + blockIdx.x] = make_double2(tb, tr);
     }
 }
 
