@@ -501,11 +501,13 @@ struct SlabZ {
 // zsafe: the ray's axial coordinates stay inside the range of the
 // magic-number floor (otherwise the caller takes the general path).  CHECK:
 // test the division's operand range here; without it the caller has shown it
-// for every slab of the ray (ray_axial).  The four candidates' addresses are
-// clamped to the volume, so that they can be loaded before the predicates
-// are known.  Voxel indices are 32-bit: volumes are validated to hold fewer
-// than 2^31 voxels (the reference indexes with int as well).
-template <bool CHECK>
+// for every slab of the ray (ray_axial).  CLAMP: the four candidates'
+// addresses are clamped to the volume, so that they can be loaded before the
+// predicates are known; otherwise they are exact only where their predicate
+// holds, and the caller loads under the predicate.  Voxel indices are
+// 32-bit: volumes are validated to hold fewer than 2^31 voxels (the
+// reference indexes with int as well).
+template <bool CHECK, bool CLAMP = true>
 __device__ __forceinline__ bool slab_window(const RayGeom &r, const Geom &g, const SlabC &c, int sz,
                                             float z_half, bool zsafe, SlabZ &w) {
     // :71-77 / :124-130 ("ratio * xc + z1 + nz / 2", z1 = 0)
@@ -513,15 +515,19 @@ __device__ __forceinline__ bool slab_window(const RayGeom &r, const Geom &g, con
     const float cz1 = __fadd_rn(__fmul_rn(r.rz1, c.dc), z_half);
     const float zi1 = fminf(cz0, cz1), zi2 = fmaxf(cz0, cz1);
     float fz0;
-    const int Z1 = mk_floor(zi1, fz0), Z2 = mk_floor_i(zi2);
-    const float fz1 = __fadd_rn(fz0, 1.0f);
+    const int Z1 = mk_floor(zi1, fz0);
+    const float fz1 = __fadd_rn(fz0, 1.0f), fz2 = __fadd_rn(fz1, 1.0f);
     const float dz = __fsub_rn(zi2, zi1);
-    const unsigned nz = (unsigned)g.nz, dZ = (unsigned)Z2 - (unsigned)Z1;
+    // Z2 = floor(zi2) is Z1 (zi2 < Z1 + 1) or Z1 + 1 (zi2 < Z1 + 2) for a
+    // window of at most two slices: compared against the exact floats
+    // Z1 + 1, Z1 + 2 (zsafe: |zi| < 2^19)
+    const bool two = zi2 >= fz1, narrow = zi2 < fz2;
+    const unsigned nz = (unsigned)g.nz;
     // the reference's axial loop visits Z1 and (when Z2 = Z1 + 1) Z1 + 1,
     // clamped to the volume (:80-82 / :133-135)
     const bool u0 = c.flags & SC_U0, u1 = c.flags & SC_U1;
     const bool z0 = (unsigned)Z1 < nz;
-    const bool z1 = dZ != 0u && (unsigned)Z1 + 1u < nz;
+    const bool z1 = two && (unsigned)Z1 + 1u < nz;
     w.p00 = u0 && z0;
     w.p01 = u0 && z1;
     w.p10 = u1 && z0;
@@ -529,18 +535,26 @@ __device__ __forceinline__ bool slab_window(const RayGeom &r, const Geom &g, con
     w.wu0 = c.a;
     w.wu1 = c.b;
     const float n0 = __fsub_rn(fminf(fz1, zi2), fmaxf(fz0, zi1));
-    const float n1 = __fsub_rn(fminf(__fadd_rn(fz1, 1.0f), zi2), fmaxf(fz1, zi1));
+    const float n1 = __fsub_rn(fminf(fz2, zi2), fmaxf(fz1, zi1));
     const float y = mk_recip(dz);
     w.wz0 = mk_div(n0, dz, y);
     w.wz1 = mk_div(n1, dz, y);
     const bool exact = CHECK ? (mk_den_ok(dz) && mk_num_ok(n0) && mk_num_ok(n1)) : true;
-    const int cz0i = min(max(Z1, 0), g.nz - 1), cz1i = min(max(Z1 + 1, 0), g.nz - 1);
-    w.a00 = c.r0 + cz0i * sz;
-    w.a01 = c.r0 + cz1i * sz;
-    w.a10 = c.r1 + cz0i * sz;
-    w.a11 = c.r1 + cz1i * sz;
+    if (CLAMP) {
+        const int cz0i = min(max(Z1, 0), g.nz - 1), cz1i = min(max(Z1 + 1, 0), g.nz - 1);
+        w.a00 = c.r0 + cz0i * sz;
+        w.a01 = c.r0 + cz1i * sz;
+        w.a10 = c.r1 + cz0i * sz;
+        w.a11 = c.r1 + cz1i * sz;
+    } else {  // (unsigned: wraps instead of overflowing where Z1 is out of range)
+        const unsigned zo = (unsigned)Z1 * (unsigned)sz;
+        w.a00 = (int)((unsigned)c.r0 + zo);
+        w.a01 = (int)((unsigned)w.a00 + (unsigned)sz);
+        w.a10 = (int)((unsigned)c.r1 + zo);
+        w.a11 = (int)((unsigned)w.a10 + (unsigned)sz);
+    }
     // outside the division's checked range the caller takes the general path
-    return (c.flags & SC_NARROW) && dZ <= 1u && exact && zsafe;
+    return (c.flags & SC_NARROW) && narrow && exact && zsafe;
 }
 
 // Per-ray facts about the axial footprint over all the ray's slabs, bounded
@@ -636,7 +650,8 @@ __device__ __forceinline__ void fp_slab(const RayGeom &r, const Geom &g, const S
                                         const VT *const *base, int su, int sd, int sz,
                                         float z_half, bool zsafe, float *acc, float &accw) {
     SlabZ w;
-    if (slab_window<CHECK>(r, g, e, sz, z_half, zsafe, w)) {
+    // (every load below is under its voxel's predicate)
+    if (slab_window<CHECK, false>(r, g, e, sz, z_half, zsafe, w)) {
 #pragma unroll
         for (int k = 0; k < K; k++) {
             if (w.p00) acc[k] = __fmaf_rn(__fmul_rn(ldv(base[k], w.a00), w.wu0), w.wz0, acc[k]);
@@ -680,27 +695,44 @@ __device__ __forceinline__ void fp_slab(const RayGeom &r, const Geom &g, const S
     }
 }
 
+// One volume: the window's voxels are loaded under their predicates from
+// unclamped addresses (fewer index instructions); with more volumes from
+// clamped addresses without predicates (fewer registers).
+#ifndef MCSART_FP_PREDLOAD
+#define MCSART_FP_PREDLOAD 1
+#endif
+template <int K> constexpr bool fp_pred_load() { return K == 1 && MCSART_FP_PREDLOAD; }
+
 // The windows of slabs d0+j .. d0+j+G-1 of a ray and the 4*K voxel
-// values of each (addresses are clamped, so every load is in bounds); true if
-// all of them are exact 2x2 windows.
+// values of each (every load is in bounds: clamped addresses, or unclamped
+// ones loaded only where the voxel is in the window); true if all of them
+// are exact 2x2 windows.
 template <int K, int G, bool CHECK, typename VT>
 __device__ __forceinline__ bool fp_group_load(const RayGeom &r, const Geom &g,
                                               const SlabC (*sm_c)[FPC_COLS], int col, int j, int sz,
                                               const VT *const *base, float z_half, bool zsafe,
                                               SlabZ *w,
                                               float (*v)[K][4]) {
+    constexpr bool pred = fp_pred_load<K>();
     bool all_fast = true;
 #pragma unroll
     for (int q = 0; q < G; q++)
-        all_fast &= slab_window<CHECK>(r, g, sm_c[j + q][col], sz, z_half, zsafe, w[q]);
+        all_fast &= slab_window<CHECK, !pred>(r, g, sm_c[j + q][col], sz, z_half, zsafe, w[q]);
 #pragma unroll
     for (int q = 0; q < G; q++)
 #pragma unroll
         for (int k = 0; k < K; k++) {
-            v[q][k][0] = ldv(base[k], w[q].a00);
-            v[q][k][1] = ldv(base[k], w[q].a01);
-            v[q][k][2] = ldv(base[k], w[q].a10);
-            v[q][k][3] = ldv(base[k], w[q].a11);
+            if (pred) {  // values outside the window are never used
+                v[q][k][0] = w[q].p00 ? ldv(base[k], w[q].a00) : 0.0f;
+                v[q][k][1] = w[q].p01 ? ldv(base[k], w[q].a01) : 0.0f;
+                v[q][k][2] = w[q].p10 ? ldv(base[k], w[q].a10) : 0.0f;
+                v[q][k][3] = w[q].p11 ? ldv(base[k], w[q].a11) : 0.0f;
+            } else {
+                v[q][k][0] = ldv(base[k], w[q].a00);
+                v[q][k][1] = ldv(base[k], w[q].a01);
+                v[q][k][2] = ldv(base[k], w[q].a10);
+                v[q][k][3] = ldv(base[k], w[q].a11);
+            }
         }
     return all_fast;
 }
