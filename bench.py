@@ -660,6 +660,13 @@ def main():
             ext = max_over_ranks(e0.elapsed_time(e1) / 1000.0)
             extras[name] = {"value": xsteps / ext * world,
                             "unit": "iterations/s"}
+            if name.startswith("subsets") or name.startswith("bf16"):
+                # where the time goes in this mode (one step, graphs bypassed)
+                ctx.profile_begin()
+                st()
+                pr_ = ctx.profile_end()
+                extras[name]["kernel_ms_per_step"] = {k: round(v[1], 2) for k, v in pr_.items()
+                                                      if v[1] >= 0.05}
 
         # four independent problems of this workload (different seeds) run
         # concurrently through mcsart_batch_run: problems per second x steps
