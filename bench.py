@@ -157,18 +157,20 @@ def algorithmic_bytes(p) -> dict:
         "bp_div": 8 * P + 4 * V,
         # read volume (+ its update), write volume and its y-fastest copy
         "bp_div_add": 8 * P + 12 * V,
-        # read img, 6 fields; write warped volume and its y-fastest copy
-        "warp_fwd": 4 * V + 24 * V + 8 * V,
+        # read img, 6 fields; write the warped volume in the layout the
+        # view's projector reads (x- or y-fastest)
+        "warp_fwd": 4 * V + 24 * V + 4 * V,
         # read ratio, 6 fields, img; write img and (texture model, the
         # default) its 3D-array copy
         "warp_back_add": 4 * V + 24 * V + 8 * V + 4 * V,
-        # read img, 6 fields; write img0, ones and their copies
-        "motion_prep": 4 * V + 24 * V + 16 * V,
+        # read img, 6 fields; write img0 and ones in the layout the view's
+        # projector reads
+        "motion_prep": 4 * V + 24 * V + 8 * V,
         # read ratio, img, read+write 6 fields
         "field_update": 8 * V + 48 * V,
         # the two above in one pass: read ratio, img, read+write 6 fields,
-        # write img0, ones and their copies
-        "field_update_prep": 8 * V + 48 * V + 16 * V,
+        # write img0 and ones in the layout the next view's projector reads
+        "field_update_prep": 8 * V + 48 * V + 8 * V,
     }
 
 
