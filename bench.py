@@ -715,7 +715,7 @@ def main():
                 "e2e": e2e, "gpu_launches": int(launches), "roofline": roofline,
                 "cpu_baseline": cpu, "clocks": clk, "kernel_ms_per_step": kernel_ms,
                 "launch_shapes": {"autotuned": bool(drop_in.autotune),
-                                  "variants_fp1_fp3_bp_warp": ctx.tuning_get(g)},
+                                  "variants_fp1_fp3_bp_warp_fup": ctx.tuning_get(g)},
                 "extras": extras}
         print(json.dumps(line), flush=True)
     ctx.close()

@@ -293,15 +293,16 @@ int mcsart_batch_run(mcsart_ctx *ctx, const mcsart_problem *problems, int n_prob
  * src/cu_backprojection.cu:46, src/cu_deform.cu:5).  Times the candidate
  * shapes of the driver's per-view kernels (projector slab-group depth and
  * blocks per SM, backprojector voxels per thread and rows per block, warp
- * rows per thread) on a sample of the problem's views (an image pass and a
+ * rows per thread, the DVF-pass field update's load order) on a sample of the problem's views (an image pass and a
  * DVF-update pass over up to 12 views, on copies of the image and fields;
  * the problem's buffers are not changed) and caches the fastest for the
  * problem's geometry and opt->storage.  Later driver runs of that geometry
  * use them.  Every candidate gives the same bits. */
 int mcsart_autotune(mcsart_ctx *ctx, const mcsart_problem *prob, const mcsart_options *opt);
-/* The cached shapes of prob's geometry and `storage` as four variant indices
- * (projector one-volume, projector three-volume, backprojector, warp; -1 =
- * built-in): returns 1 and fills shapes[4], or 0 if none are cached. */
+/* The cached shapes of prob's geometry and `storage` as five variant indices
+ * (projector one-volume, projector three-volume, backprojector, warp, DVF-pass
+ * field update; -1 = built-in): returns 1 and fills shapes[5], or 0 if none
+ * are cached. */
 int mcsart_tuning_get(mcsart_ctx *ctx, const mcsart_problem *prob, int storage, int *shapes);
 /* Write / read the context's tuning cache as a text file (one geometry per
  * line); load returns the number of entries read. */

@@ -59,6 +59,7 @@ struct Tuning {
     int fp3 = -1;   // three-volume projector (DVF-update passes)
     int bp = -1;    // backprojector: voxels per thread along z, voxel rows per block
     int warp = -1;  // image-pass warps: voxel rows per thread
+    int fup = -1;   // DVF-pass field update + prep: field loads voxel by voxel or early
 };
 
 }  // namespace mcsart

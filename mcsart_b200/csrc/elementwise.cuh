@@ -288,7 +288,11 @@ static __global__ void __launch_bounds__(256) field_update_kernel(FT *ax, FT *ay
 // values in shared memory and then computes img0 / ones of tile A for the
 // next view.  Every field voxel is updated by exactly one block, and the
 // arithmetic is that of the two kernels, so the results are bitwise theirs.
-template <typename FT, typename VT>
+// EARLY (a launch shape the driver's tuning may choose): every thread loads
+// its 4 x 6 field values first, before the ratio tile and its barrier, so
+// that 24 loads per thread are in flight at once (more registers, fewer
+// resident blocks); otherwise the fields are loaded voxel by voxel.
+template <typename FT, typename VT, bool EARLY = false>
 static __global__ void __launch_bounds__(256) field_update_prep_kernel(
     FT *ax, FT *ay, FT *az, FT *bx, FT *by, FT *bz, const float *img_temp, const float *img,
     int nx, int ny, int nz, float nvd, float nfd, VT *img0, VT *img0T, VT *ones, VT *onesT,
@@ -299,6 +303,22 @@ static __global__ void __launch_bounds__(256) field_update_prep_kernel(
     const int tx = threadIdx.x, ty = threadIdx.y;
     const int x0 = blockIdx.x * 32, y0 = blockIdx.y * 32, iz = blockIdx.z;
     const int64_t slice = (int64_t)iz * nx * ny;
+    // the field values at this thread's 4 voxels of A^T (EARLY)
+    float fe[EARLY ? 4 : 1][6];
+    if (EARLY) {
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const int lx = ty + 8 * k, xp = y0 + tx, yp = x0 + lx;
+            const bool in = xp < nx && yp < ny;
+            const int64_t id = in ? xp + (int64_t)yp * nx + slice : 0;
+            fe[k][0] = in ? ldv(ay, id) : 0.0f;
+            fe[k][1] = in ? ldv(ax, id) : 0.0f;
+            fe[k][2] = in ? ldv(az, id) : 0.0f;
+            fe[k][3] = in ? ldv(by, id) : 0.0f;
+            fe[k][4] = in ? ldv(bx, id) : 0.0f;
+            fe[k][5] = in ? ldv(bz, id) : 0.0f;
+        }
+    }
     // ratio on tile A, x-fastest: rt[y - y0][x - x0]
 #pragma unroll
     for (int k = 0; k < 4; k++) {
@@ -319,12 +339,18 @@ static __global__ void __launch_bounds__(256) field_update_prep_kernel(
             const float dfy = fwd_diff(img, id, v, nx, ny, nz, 2);
             const float dfz = fwd_diff(img, id, v, nx, ny, nz, 3);
             const float q = rt[tx][lx];
-            const FT nay = cvt<FT>(__fmaf_rn(q * nvd, dfx, ldv(ay, id)));
-            const FT nax = cvt<FT>(__fmaf_rn(q * nvd, dfy, ldv(ax, id)));
-            const FT naz = cvt<FT>(__fmaf_rn(q * nvd, dfz, ldv(az, id)));
-            const FT nby = cvt<FT>(__fmaf_rn(q * nfd, dfx, ldv(by, id)));
-            const FT nbx = cvt<FT>(__fmaf_rn(q * nfd, dfy, ldv(bx, id)));
-            const FT nbz = cvt<FT>(__fmaf_rn(q * nfd, dfz, ldv(bz, id)));
+            const float fay = EARLY ? fe[k % (EARLY ? 4 : 1)][0] : ldv(ay, id);
+            const float fax = EARLY ? fe[k % (EARLY ? 4 : 1)][1] : ldv(ax, id);
+            const float faz = EARLY ? fe[k % (EARLY ? 4 : 1)][2] : ldv(az, id);
+            const float fby = EARLY ? fe[k % (EARLY ? 4 : 1)][3] : ldv(by, id);
+            const float fbx = EARLY ? fe[k % (EARLY ? 4 : 1)][4] : ldv(bx, id);
+            const float fbz = EARLY ? fe[k % (EARLY ? 4 : 1)][5] : ldv(bz, id);
+            const FT nay = cvt<FT>(__fmaf_rn(q * nvd, dfx, fay));
+            const FT nax = cvt<FT>(__fmaf_rn(q * nvd, dfy, fax));
+            const FT naz = cvt<FT>(__fmaf_rn(q * nvd, dfz, faz));
+            const FT nby = cvt<FT>(__fmaf_rn(q * nfd, dfx, fby));
+            const FT nbx = cvt<FT>(__fmaf_rn(q * nfd, dfy, fbx));
+            const FT nbz = cvt<FT>(__fmaf_rn(q * nfd, dfz, fbz));
             ay[id] = nay; ax[id] = nax; az[id] = naz;
             by[id] = nby; bx[id] = nbx; bz[id] = nbz;
             n[0] = tof(nay); n[1] = tof(nax); n[2] = tof(naz);

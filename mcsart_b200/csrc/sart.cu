@@ -182,22 +182,30 @@ template <typename ST, int INTERP, int SUM> struct Runner {
         if (SUM == SUM_REF && K == 1) {
             // built-in: deeper slab groups when every block is resident at once
             const int var = tune.fp1 >= 0 ? tune.fp1 : fp_one_wave(ctx, fp_bx, fp_by) ? 1 : 0;
-            if (var == 1)
-                MC_LAUNCH(ctx, (fp_ref_kernel<K, ONES, VT, ST, false, 4, 4>), grid,
-                          dim3(FPC_THREADS), 0, a);
-            else if (var == 2)
-                MC_LAUNCH(ctx, (fp_ref_kernel<K, ONES, VT, ST, false, 1, 8>), grid,
-                          dim3(FPC_THREADS), 0, a);
-            else
-                MC_LAUNCH(ctx, (fp_ref_kernel<K, ONES, VT, ST, false, 2, 6>), grid,
-                          dim3(FPC_THREADS), 0, a);
+            // (slab-group depth, resident blocks per SM)
+            switch (var) {
+                case 1: MC_LAUNCH(ctx, (fp_ref_kernel<K, ONES, VT, ST, false, 4, 4>), grid,
+                                  dim3(FPC_THREADS), 0, a); break;
+                case 2: MC_LAUNCH(ctx, (fp_ref_kernel<K, ONES, VT, ST, false, 1, 8>), grid,
+                                  dim3(FPC_THREADS), 0, a); break;
+                case 3: MC_LAUNCH(ctx, (fp_ref_kernel<K, ONES, VT, ST, false, 2, 7>), grid,
+                                  dim3(FPC_THREADS), 0, a); break;
+                case 4: MC_LAUNCH(ctx, (fp_ref_kernel<K, ONES, VT, ST, false, 4, 5>), grid,
+                                  dim3(FPC_THREADS), 0, a); break;
+                default: MC_LAUNCH(ctx, (fp_ref_kernel<K, ONES, VT, ST, false, 2, 6>), grid,
+                                   dim3(FPC_THREADS), 0, a);
+            }
         } else if (SUM == SUM_REF) {
-            if (tune.fp3 == 1)
-                MC_LAUNCH(ctx, (fp_ref_kernel<K, ONES, VT, ST, false, 2, 4>), grid,
-                          dim3(FPC_THREADS), 0, a);
-            else
-                MC_LAUNCH(ctx, (fp_ref_kernel<K, ONES, VT, ST, false, 4, 4>), grid,
-                          dim3(FPC_THREADS), 0, a);
+            switch (tune.fp3) {
+                case 1: MC_LAUNCH(ctx, (fp_ref_kernel<K, ONES, VT, ST, false, 2, 4>), grid,
+                                  dim3(FPC_THREADS), 0, a); break;
+                case 2: MC_LAUNCH(ctx, (fp_ref_kernel<K, ONES, VT, ST, false, 2, 5>), grid,
+                                  dim3(FPC_THREADS), 0, a); break;
+                case 3: MC_LAUNCH(ctx, (fp_ref_kernel<K, ONES, VT, ST, false, 4, 5>), grid,
+                                  dim3(FPC_THREADS), 0, a); break;
+                default: MC_LAUNCH(ctx, (fp_ref_kernel<K, ONES, VT, ST, false, 4, 4>), grid,
+                                   dim3(FPC_THREADS), 0, a);
+            }
         } else if (opt.geom64) {
             const size_t smem = (size_t)groups * (K + 1) * 32 * sizeof(float);
             MC_LAUNCH(ctx, (fp_kernel<K, ONES, SUM == SUM_REF ? SUM_PLAIN : SUM, VT, ST, true>),
@@ -557,11 +565,20 @@ template <typename ST, int INTERP, int SUM> struct Runner {
                 const float vdn = P.volumes[vn] - P.volumes[vn - 1];
                 const float fdn = P.flows[vn] - P.flows[vn - 1];
                 ctx->label = "field_update_prep";
-                MC_LAUNCH(ctx, (field_update_prep_kernel<ST, ST>), tile_grid(), dim3(32, 8), 0,
-                          fw, fw + V, fw + 2 * V, fw + 3 * V, fw + 4 * V, fw + 5 * V,
-                          (const float *)S.ratio.as<float>(), (const float *)P.img, g.nx, g.ny,
-                          g.nz, nvd, nfd, std_or_null(vn, S.img0), tr_or_null(vn, S.img0T),
-                          std_or_null(vn, S.ones), tr_or_null(vn, S.onesT), vdn, fdn);
+                if (tune.fup == 1)
+                    MC_LAUNCH(ctx, (field_update_prep_kernel<ST, ST, true>), tile_grid(),
+                              dim3(32, 8), 0, fw, fw + V, fw + 2 * V, fw + 3 * V, fw + 4 * V,
+                              fw + 5 * V, (const float *)S.ratio.as<float>(), (const float *)P.img,
+                              g.nx, g.ny, g.nz, nvd, nfd, std_or_null(vn, S.img0),
+                              tr_or_null(vn, S.img0T), std_or_null(vn, S.ones),
+                              tr_or_null(vn, S.onesT), vdn, fdn);
+                else
+                    MC_LAUNCH(ctx, (field_update_prep_kernel<ST, ST>), tile_grid(), dim3(32, 8),
+                              0, fw, fw + V, fw + 2 * V, fw + 3 * V, fw + 4 * V, fw + 5 * V,
+                              (const float *)S.ratio.as<float>(), (const float *)P.img, g.nx,
+                              g.ny, g.nz, nvd, nfd, std_or_null(vn, S.img0),
+                              tr_or_null(vn, S.img0T), std_or_null(vn, S.ones),
+                              tr_or_null(vn, S.onesT), vdn, fdn);
             } else {
                 ctx->label = "field_update";
                 MC_LAUNCH(ctx, (field_update_kernel<ST>), tile_grid(), dim3(32, 8), 0, fw, fw + V,
@@ -588,9 +605,9 @@ template <typename ST, int INTERP, int SUM> struct Runner {
             k.insert(k.end(), b, b + n);
         };
         // the storage type itself, not its size: BF16 and F16 are both 2 bytes
-        const int hdr[14] = {kind, opt.storage, INTERP, SUM, groups, (int)P.motion_model,
+        const int hdr[15] = {kind, opt.storage, INTERP, SUM, groups, (int)P.motion_model,
                              (int)views_mot.size(), subset, inv_iters, opt.geom64,
-                             tune.fp1, tune.fp3, tune.bp, tune.warp};
+                             tune.fp1, tune.fp3, tune.bp, tune.warp, tune.fup};
         put(hdr, sizeof(hdr));
         put(views_img.data(), views_img.size() * sizeof(int));
         put(views_mot.data(), views_mot.size() * sizeof(int));

@@ -28,13 +28,14 @@
 namespace mcsart {
 
 // Variant counts of each kernel class (the launches are in sart.cu's Runner):
-//   fp1  one-volume projector   0: 2-slab groups, 6 blocks/SM   1: 4-slab groups, 4 blocks/SM
-//                               2: 1-slab groups, 8 blocks/SM
-//   fp3  three-volume projector 0: 4-slab groups, 4 blocks/SM   1: 2-slab groups, 4 blocks/SM
+//   fp1  one-volume projector   (slab-group depth, resident blocks per SM)
+//                               0: (2, 6)  1: (4, 4)  2: (1, 8)  3: (2, 7)  4: (4, 5)
+//   fp3  three-volume projector 0: (4, 4)  1: (2, 4)  2: (2, 5)  3: (4, 5)
 //   bp   backprojector          0: 2 voxels/thread, 4 rows      1: 1 voxel, 4 rows
 //                               2: 2 voxels, 8 rows             3: 4 voxels, 4 rows
 //   warp image-pass warps       0: 2 rows/thread  1: 1 row  2: 4 rows
-constexpr int N_FP1 = 3, N_FP3 = 2, N_BP = 4, N_WARP = 3;
+//   fup  DVF-pass field update  0: fields loaded voxel by voxel  1: all loaded first
+constexpr int N_FP1 = 5, N_FP3 = 4, N_BP = 4, N_WARP = 3, N_FUP = 2;
 
 std::string tuning_key(const Geom &g, int storage) {
     char b[256];
@@ -97,9 +98,10 @@ int autotune_problem(mcsart_ctx *ctx, const Problem &P, const mcsart_options &op
     opt.autotune = 0;
     const int op[2] = {1, 0};
 
-    const int n_trials = std::max(std::max(N_FP1, N_FP3), std::max(N_BP, N_WARP));
+    const int n_trials =
+        std::max(std::max(std::max(N_FP1, N_FP3), std::max(N_BP, N_WARP)), N_FUP);
     std::vector<double> best_fp1(N_FP1, 1e30), best_fp3(N_FP3, 1e30), best_bp(N_BP, 1e30),
-        best_warp(N_WARP, 1e30);
+        best_warp(N_WARP, 1e30), best_fup(N_FUP, 1e30);
     int rc = MCSART_OK;
     for (int round = 0; round < 2 && rc == MCSART_OK; round++) {
         for (int t = 0; t < n_trials && rc == MCSART_OK; t++) {
@@ -108,6 +110,7 @@ int autotune_problem(mcsart_ctx *ctx, const Problem &P, const mcsart_options &op
             trial.fp3 = t % N_FP3;
             trial.bp = t % N_BP;
             trial.warp = t % N_WARP;
+            trial.fup = t % N_FUP;
             MC_CHECK_CUDA(cudaMemcpyAsync(img_ws, P.img, V * sizeof(float),
                                           cudaMemcpyDeviceToDevice, ctx->stream));
             MC_CHECK_CUDA(cudaMemcpyAsync(f_ws, P.fields, 6 * V * es, cudaMemcpyDeviceToDevice,
@@ -123,10 +126,12 @@ int autotune_problem(mcsart_ctx *ctx, const Problem &P, const mcsart_options &op
             const double f3 = per_launch(ctx, {"fp_motion"});
             const double b = per_launch(ctx, {"bp_div", "bp_div_add"});
             const double w = per_launch(ctx, {"warp_fwd", "warp_back_add"});
+            const double u = per_launch(ctx, {"field_update_prep"});
             if (f1 >= 0) best_fp1[trial.fp1] = std::min(best_fp1[trial.fp1], f1);
             if (f3 >= 0) best_fp3[trial.fp3] = std::min(best_fp3[trial.fp3], f3);
             if (b >= 0) best_bp[trial.bp] = std::min(best_bp[trial.bp], b);
             if (w >= 0) best_warp[trial.warp] = std::min(best_warp[trial.warp], w);
+            if (u >= 0) best_fup[trial.fup] = std::min(best_fup[trial.fup], u);
         }
     }
     ctx->prof_table.clear();
@@ -141,6 +146,7 @@ int autotune_problem(mcsart_ctx *ctx, const Problem &P, const mcsart_options &op
     best.fp3 = argmin(best_fp3);
     best.bp = argmin(best_bp);
     best.warp = argmin(best_warp);
+    best.fup = argmin(best_fup);
     ctx->tuning[tuning_key(P.g, opt_in.storage)] = best;
     MC_CHECK_CUDA(cudaStreamSynchronize(ctx->stream));
     return MCSART_OK;
@@ -165,6 +171,7 @@ MC_EXPORT int mcsart_tuning_get(mcsart_ctx *ctx, const mcsart_problem *prob, int
     shapes[1] = it->second.fp3;
     shapes[2] = it->second.bp;
     shapes[3] = it->second.warp;
+    shapes[4] = it->second.fup;
     return 1;
 }
 
@@ -174,10 +181,10 @@ MC_EXPORT int mcsart_tuning_save(mcsart_ctx *ctx, const char *path) {
     MC_REQUIRE(path, "path is NULL");
     FILE *f = fopen(path, "w");
     MC_REQUIRE(f, "cannot open %s for writing", path);
-    fprintf(f, "# mcsart tuning cache v1: key fp1 fp3 bp warp\n");
+    fprintf(f, "# mcsart tuning cache v2: key fp1 fp3 bp warp fup\n");
     for (const auto &e : ctx->tuning)
-        fprintf(f, "%s %d %d %d %d\n", e.first.c_str(), e.second.fp1, e.second.fp3, e.second.bp,
-                e.second.warp);
+        fprintf(f, "%s %d %d %d %d %d\n", e.first.c_str(), e.second.fp1, e.second.fp3,
+                e.second.bp, e.second.warp, e.second.fup);
     const bool ok = fclose(f) == 0;
     MC_REQUIRE(ok, "writing %s failed", path);
     return MCSART_OK;
@@ -195,9 +202,10 @@ MC_EXPORT int mcsart_tuning_load(mcsart_ctx *ctx, const char *path) {
         if (line[0] == '#' || line[0] == '\n') continue;
         char key[400];
         Tuning t;
-        if (sscanf(line, "%399s %d %d %d %d", key, &t.fp1, &t.fp3, &t.bp, &t.warp) != 5 ||
+        if (sscanf(line, "%399s %d %d %d %d %d", key, &t.fp1, &t.fp3, &t.bp, &t.warp, &t.fup) !=
+                6 ||
             t.fp1 < -1 || t.fp1 >= N_FP1 || t.fp3 < -1 || t.fp3 >= N_FP3 || t.bp < -1 ||
-            t.bp >= N_BP || t.warp < -1 || t.warp >= N_WARP) {
+            t.bp >= N_BP || t.warp < -1 || t.warp >= N_WARP || t.fup < -1 || t.fup >= N_FUP) {
             bad++;
             continue;
         }

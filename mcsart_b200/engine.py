@@ -394,7 +394,7 @@ class Context:
     def autotune(self, *, geo, n_views, lambda_, angles, volumes, flows, img, proj, fields=None,
                  options=None) -> list:
         """mcsart_autotune for one problem (same keyword arguments as
-        aumisart_device); returns the cached variant indices [fp1, fp3, bp, warp]."""
+        aumisart_device); returns the cached variant indices [fp1, fp3, bp, warp, fup]."""
         p, keep = self._problem(geo, n_views, lambda_, angles, volumes, flows, img, proj, fields,
                                 None, None, options)
         self._call("mcsart_autotune", ctypes.byref(p),
@@ -403,13 +403,13 @@ class Context:
         return self.tuning_get(geo, storage)
 
     def tuning_get(self, geo, storage=F32):
-        """Cached launch-shape variants [fp1, fp3, bp, warp] of a geometry, or None."""
+        """Cached launch-shape variants [fp1, fp3, bp, warp, fup] of a geometry, or None."""
         p = Problem()
         p.nx, p.ny, p.nz = int(geo["nx"]), int(geo["ny"]), int(geo["nz"])
         p.na, p.nb = int(geo["na"]), int(geo["nb"])
         p.SO, p.SD, p.da, p.db = geo["SO"], geo["SD"], geo["da"], geo["db"]
         p.ai, p.bi = geo["ai"], geo["bi"]
-        out = (ctypes.c_int * 4)()
+        out = (ctypes.c_int * 5)()
         rc = self._L.mcsart_tuning_get(self._h, ctypes.byref(p), int(storage), out)
         if rc < 0:
             check(rc, "mcsart_tuning_get")

@@ -13,7 +13,7 @@ from test_gpu_sart import make_case
 
 pytestmark = pytest.mark.gpu
 
-N_VARIANTS = (3, 2, 4, 3)  # fp1, fp3, bp, warp
+N_VARIANTS = (5, 4, 4, 3, 2)  # fp1, fp3, bp, warp, fup
 
 
 def _run(ctx, torch, case, opt):
@@ -46,7 +46,7 @@ def test_autotune_caches_shapes_and_keeps_the_bits(ctx, torch_cuda, oracle, tmp_
     shapes = ctx.autotune(**prob)
     # the problem's own buffers are left as they were
     np.testing.assert_array_equal(host(prob["img"]), img_before)
-    assert shapes is not None and len(shapes) == 4
+    assert shapes is not None and len(shapes) == 5
     for s, n in zip(shapes, N_VARIANTS):
         assert -1 <= s < n
     tuned = _run(ctx, torch, case, m.default_options())
@@ -79,10 +79,10 @@ def test_every_launch_shape_gives_the_same_bits(ctx, torch_cuda, oracle, tmp_pat
     combos = set()
     for cls, n in enumerate(N_VARIANTS):  # each variant of each class at least once
         for v in range(n):
-            shape = [-1, -1, -1, -1]
+            shape = [-1, -1, -1, -1, -1]
             shape[cls] = v
             combos.add(tuple(shape))
-    combos |= {tuple(v % n for n in N_VARIANTS) for v in range(4)}
+    combos |= {tuple(v % n for n in N_VARIANTS) for v in range(5)}
     for shape in sorted(combos):
         p = tmp_path / "forced.txt"
         p.write_text(f"{key} {' '.join(map(str, shape))}\n")
@@ -111,6 +111,6 @@ def test_autotune_option_tunes_on_first_run(ctx, torch_cuda, oracle):
 def test_malformed_tuning_file_is_rejected(ctx, tmp_path):
     import mcsart_b200 as m
     p = tmp_path / "bad.txt"
-    p.write_text("somekey 9 0 0 0\n")
+    p.write_text("somekey 9 0 0 0 0\n")
     with pytest.raises(m.McsartError):
         ctx.tuning_load(p)
