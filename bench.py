@@ -174,19 +174,19 @@ def algorithmic_bytes(p) -> dict:
     }
 
 
-# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per launch of the
-# workloads' kernels, from one ncu capture of each (cold cache, FP32
-# storage); summaries with the commands are kept under profiles/.
+# DRAM bytes per launch of the workload's kernels (dram__bytes.sum.per_second
+# x gpu__time_duration.sum), from one ncu capture of each in the benchmark
+# step (cold cache, FP32 storage, built-in launch shapes); summaries with the
+# commands are kept under profiles/.
 NCU_DRAM_BYTES = {
-    "c2": {"fp_motion": 15459328 + 0, "fp_image": 5316864 + 0, "bp_div": 734208 + 0,
-           "field_update_prep": 50349824 + 5771264},
-    "c3": {},
+    "c3": {"fp_motion": 132488704, "fp_image": 42956032, "bp_div": 2872064,
+           "field_update_prep": 613819647},
 }
 
 # Issue-slot utilisation (smsp__issue_active) of the projector and
 # backprojector from the same captures: these kernels are bound by issue and
 # latency, not by HBM.
-NCU_ISSUE_ACTIVE = {"c2": {"fp_image": 0.428, "fp_motion": 0.435, "bp_div": 0.743}, "c3": {}}
+NCU_ISSUE_ACTIVE = {"c3": {"fp_image": 0.570, "fp_motion": 0.606, "bp_div": 0.803}}
 
 # Views per pass of the CPU samples: the engine line's cpu_baseline leg
 # (about 10 s of CPU work) and each step of the reference arm (a few seconds,
