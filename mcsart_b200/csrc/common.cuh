@@ -205,6 +205,30 @@ template <> __device__ __forceinline__ float ldv<__nv_bfloat16>(const __nv_bfloa
 template <> __device__ __forceinline__ float ldv<__half>(const __half *p, int64_t i) {
     return __half2float(__ldg(p + i));
 }
+// Two consecutive storage-type values p[2i], p[2i+1] (8-byte aligned for
+// FP32) as one load.
+template <typename T> __device__ __forceinline__ float2 ldv2(const T *p, int64_t i);
+template <> __device__ __forceinline__ float2 ldv2<float>(const float *p, int64_t i) {
+    return __ldg(reinterpret_cast<const float2 *>(p) + i);
+}
+template <>
+__device__ __forceinline__ float2 ldv2<__nv_bfloat16>(const __nv_bfloat16 *p, int64_t i) {
+    return __bfloat1622float2(__ldg(reinterpret_cast<const __nv_bfloat162 *>(p) + i));
+}
+template <> __device__ __forceinline__ float2 ldv2<__half>(const __half *p, int64_t i) {
+    return __half22float2(__ldg(reinterpret_cast<const __half2 *>(p) + i));
+}
+// Stores (a, b) at p[2i], p[2i+1] as one two-element store.
+__device__ __forceinline__ void stv2(float *p, int64_t i, float a, float b) {
+    reinterpret_cast<float2 *>(p)[i] = make_float2(a, b);
+}
+__device__ __forceinline__ void stv2(__nv_bfloat16 *p, int64_t i, float a, float b) {
+    reinterpret_cast<__nv_bfloat162 *>(p)[i] = __floats2bfloat162_rn(a, b);
+}
+__device__ __forceinline__ void stv2(__half *p, int64_t i, float a, float b) {
+    reinterpret_cast<__half2 *>(p)[i] = __floats2half2_rn(a, b);
+}
+
 // A storage-type value as float (a value, not a load).
 __device__ __forceinline__ float tof(float v) { return v; }
 __device__ __forceinline__ float tof(__nv_bfloat16 v) { return __bfloat162float(v); }

@@ -187,8 +187,10 @@ __device__ __forceinline__ void load_tile_T(float (*tile)[33], const T *src, int
 //   ones = (dx + dy + dz img) * (-vd + -fd)
 // each written x-fastest (img0, ones) and as a y-fastest copy (img0T,
 // onesT) for the projector; either pair may be nullptr when the view's
-// projector reads only the other.
-template <typename FT, typename VT>
+// projector reads only the other.  PAIR: img0 and ones interleaved in img0
+// (img0[2i], img0[2i + 1]) and img0T, for the projector's paired load; ones
+// and onesT unused.
+template <typename FT, typename VT, bool PAIR = false>
 static __global__ void __launch_bounds__(256) motion_prep_kernel(VT *img0, VT *img0T, VT *ones,
                                                           VT *onesT, const float *img,
                                                           Fields<FT> f, int nx, int ny, int nz,
@@ -226,8 +228,12 @@ static __global__ void __launch_bounds__(256) motion_prep_kernel(VT *img0, VT *i
             a = __fmaf_rn(ft[5][tx][ly] * fd, dfz, a);
             b = (dfx + dfy + dfz) * s_ones;  // cu_initial.cu:48
             if (img0) {
-                img0[id] = cvt<VT>(a);
-                ones[id] = cvt<VT>(b);
+                if (PAIR) {
+                    stv2(img0, id, a, b);
+                } else {
+                    img0[id] = cvt<VT>(a);
+                    ones[id] = cvt<VT>(b);
+                }
             }
         }
         o0[ly][tx] = a;
@@ -240,8 +246,12 @@ static __global__ void __launch_bounds__(256) motion_prep_kernel(VT *img0, VT *i
         const int lx = ty + 8 * k, ixT = x0 + lx, iyT = y0 + tx;
         if (ixT < nx && iyT < ny) {
             const int64_t t = iyT + (int64_t)ixT * ny + slice;
-            img0T[t] = cvt<VT>(o0[tx][lx]);
-            onesT[t] = cvt<VT>(o1[tx][lx]);
+            if (PAIR) {
+                stv2(img0T, t, o0[tx][lx], o1[tx][lx]);
+            } else {
+                img0T[t] = cvt<VT>(o0[tx][lx]);
+                onesT[t] = cvt<VT>(o1[tx][lx]);
+            }
         }
     }
 }
@@ -292,7 +302,8 @@ static __global__ void __launch_bounds__(256) field_update_kernel(FT *ax, FT *ay
 // its 4 x 6 field values first, before the ratio tile and its barrier, so
 // that 24 loads per thread are in flight at once (more registers, fewer
 // resident blocks); otherwise the fields are loaded voxel by voxel.
-template <typename FT, typename VT, bool EARLY = false>
+// PAIR: img0 and ones interleaved, as in motion_prep_kernel.
+template <typename FT, typename VT, bool EARLY = false, bool PAIR = false>
 static __global__ void __launch_bounds__(256) field_update_prep_kernel(
     FT *ax, FT *ay, FT *az, FT *bx, FT *by, FT *bz, const float *img_temp, const float *img,
     int nx, int ny, int nz, float nvd, float nfd, VT *img0, VT *img0T, VT *ones, VT *onesT,
@@ -381,8 +392,12 @@ static __global__ void __launch_bounds__(256) field_update_prep_kernel(
             a = __fmaf_rn(ft[5][tx][ly] * fd, dfz, a);
             b = (dfx + dfy + dfz) * s_ones;  // cu_initial.cu:48
             if (img0) {
-                img0[id] = cvt<VT>(a);
-                ones[id] = cvt<VT>(b);
+                if (PAIR) {
+                    stv2(img0, id, a, b);
+                } else {
+                    img0[id] = cvt<VT>(a);
+                    ones[id] = cvt<VT>(b);
+                }
             }
         }
         o0[ly][tx] = a;
@@ -395,8 +410,12 @@ static __global__ void __launch_bounds__(256) field_update_prep_kernel(
         const int lx = ty + 8 * k, ixT = x0 + lx, iyT = y0 + tx;
         if (ixT < nx && iyT < ny) {
             const int64_t t = iyT + (int64_t)ixT * ny + slice;
-            img0T[t] = cvt<VT>(o0[tx][lx]);
-            onesT[t] = cvt<VT>(o1[tx][lx]);
+            if (PAIR) {
+                stv2(img0T, t, o0[tx][lx], o1[tx][lx]);
+            } else {
+                img0T[t] = cvt<VT>(o0[tx][lx]);
+                onesT[t] = cvt<VT>(o1[tx][lx]);
+            }
         }
     }
 }

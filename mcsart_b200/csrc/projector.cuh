@@ -87,6 +87,23 @@ template <typename VT, int K> struct FPVolumes {
     const VT *tr[K];   // y-fastest copies (tr[k][iy + ix*ny + iz*nx*ny]) or nullptr
 };
 
+// The K volumes' values at voxel offset a into t[0..K-1]: one load per
+// volume, or (PAIR, three volumes) the second and third interleaved in one
+// array, base[1][2a], base[1][2a + 1], read with one two-element load.
+template <int K, bool PAIR, typename VT>
+__device__ __forceinline__ void fp_voxel(const VT *const *base, int64_t a, float *t) {
+    static_assert(!PAIR || K == 3, "paired volumes come with three volumes");
+    if (PAIR) {
+        t[0] = ldv(base[0], a);
+        const float2 q = ldv2(base[1], a);
+        t[1] = q.x;
+        t[2] = q.y;
+    } else {
+#pragma unroll
+        for (int k = 0; k < K; k++) t[k] = ldv(base[k], a);
+    }
+}
+
 // Ray-sum order.  SUM_REF accumulates every voxel term straight into the ray
 // sum in the reference's order (slabs, then in-plane, then axial index,
 // acc = fma(v*w_u, w_z, acc), cu_projection.cu:81-88), so that results are
@@ -645,19 +662,35 @@ __device__ __forceinline__ void ray_zrange(const RayGeom &r, float z_half, int n
 
 // One slab of one ray, any footprint: the 2x2 window with predication or the
 // reference's loops (:80-88 / :133-141).
-template <int K, bool ONES, typename VT, bool CHECK>
+template <int K, bool ONES, typename VT, bool CHECK, bool PAIR = false>
 __device__ __forceinline__ void fp_slab(const RayGeom &r, const Geom &g, const SlabC &e, int d,
                                         const VT *const *base, int su, int sd, int sz,
                                         float z_half, bool zsafe, float *acc, float &accw) {
     SlabZ w;
     // (every load below is under its voxel's predicate)
     if (slab_window<CHECK, false>(r, g, e, sz, z_half, zsafe, w)) {
+        // each volume's terms in the window's order (the volumes' sums are
+        // independent, so visiting the voxels outermost keeps every order)
+        float t[K];
+        if (w.p00) {
+            fp_voxel<K, PAIR>(base, w.a00, t);
 #pragma unroll
-        for (int k = 0; k < K; k++) {
-            if (w.p00) acc[k] = __fmaf_rn(__fmul_rn(ldv(base[k], w.a00), w.wu0), w.wz0, acc[k]);
-            if (w.p01) acc[k] = __fmaf_rn(__fmul_rn(ldv(base[k], w.a01), w.wu0), w.wz1, acc[k]);
-            if (w.p10) acc[k] = __fmaf_rn(__fmul_rn(ldv(base[k], w.a10), w.wu1), w.wz0, acc[k]);
-            if (w.p11) acc[k] = __fmaf_rn(__fmul_rn(ldv(base[k], w.a11), w.wu1), w.wz1, acc[k]);
+            for (int k = 0; k < K; k++) acc[k] = __fmaf_rn(__fmul_rn(t[k], w.wu0), w.wz0, acc[k]);
+        }
+        if (w.p01) {
+            fp_voxel<K, PAIR>(base, w.a01, t);
+#pragma unroll
+            for (int k = 0; k < K; k++) acc[k] = __fmaf_rn(__fmul_rn(t[k], w.wu0), w.wz1, acc[k]);
+        }
+        if (w.p10) {
+            fp_voxel<K, PAIR>(base, w.a10, t);
+#pragma unroll
+            for (int k = 0; k < K; k++) acc[k] = __fmaf_rn(__fmul_rn(t[k], w.wu1), w.wz0, acc[k]);
+        }
+        if (w.p11) {
+            fp_voxel<K, PAIR>(base, w.a11, t);
+#pragma unroll
+            for (int k = 0; k < K; k++) acc[k] = __fmaf_rn(__fmul_rn(t[k], w.wu1), w.wz1, acc[k]);
         }
         if (ONES) {
             if (w.p00) accw = __fmaf_rn(w.wu0, w.wz0, accw);
@@ -687,9 +720,10 @@ __device__ __forceinline__ void fp_slab(const RayGeom &r, const Geom &g, const S
             const float wz = __fdiv_rn(__fsub_rn(fminf(__fadd_rn((float)z, 1.0f), zi2),
                                                  fmaxf((float)z, zi1)), dz);
             const int a = rowa + z * sz;
+            float t[K];
+            fp_voxel<K, PAIR>(base, a, t);
 #pragma unroll
-            for (int k = 0; k < K; k++)
-                acc[k] = __fmaf_rn(__fmul_rn(ldv(base[k], a), wu), wz, acc[k]);
+            for (int k = 0; k < K; k++) acc[k] = __fmaf_rn(__fmul_rn(t[k], wu), wz, acc[k]);
             if (ONES) accw = __fmaf_rn(wu, wz, accw);
         }
     }
@@ -700,7 +734,7 @@ __device__ __forceinline__ void fp_slab(const RayGeom &r, const Geom &g, const S
 // be issued before the predicates are known; loading under the predicates
 // from unclamped addresses measured 2-3 % slower at 256x256x160); true if
 // all of them are exact 2x2 windows.
-template <int K, int G, bool CHECK, typename VT>
+template <int K, int G, bool CHECK, typename VT, bool PAIR = false>
 __device__ __forceinline__ bool fp_group_load(const RayGeom &r, const Geom &g,
                                               const SlabC (*sm_c)[FPC_COLS], int col, int j, int sz,
                                               const VT *const *base, float z_half, bool zsafe,
@@ -711,20 +745,22 @@ __device__ __forceinline__ bool fp_group_load(const RayGeom &r, const Geom &g,
     for (int q = 0; q < G; q++)
         all_fast &= slab_window<CHECK>(r, g, sm_c[j + q][col], sz, z_half, zsafe, w[q]);
 #pragma unroll
-    for (int q = 0; q < G; q++)
+    for (int q = 0; q < G; q++) {
+        const int a[4] = {w[q].a00, w[q].a01, w[q].a10, w[q].a11};
 #pragma unroll
-        for (int k = 0; k < K; k++) {
-            v[q][k][0] = ldv(base[k], w[q].a00);
-            v[q][k][1] = ldv(base[k], w[q].a01);
-            v[q][k][2] = ldv(base[k], w[q].a10);
-            v[q][k][3] = ldv(base[k], w[q].a11);
+        for (int i = 0; i < 4; i++) {
+            float t[K];
+            fp_voxel<K, PAIR>(base, a[i], t);
+#pragma unroll
+            for (int k = 0; k < K; k++) v[q][k][i] = t[k];
         }
+    }
     return all_fast;
 }
 
 // The terms of one group in the reference's order: from the loaded windows
 // when all are 2x2 (fast), else slab by slab on the general path.
-template <int K, int G, bool ONES, typename VT, bool CHECK>
+template <int K, int G, bool ONES, typename VT, bool CHECK, bool PAIR = false>
 __device__ __forceinline__ void fp_group_sum(const RayGeom &r, const Geom &g,
                                              const SlabC (*sm_c)[FPC_COLS], int col, int j, int d0,
                                              const VT *const *base, int su, int sd, int sz,
@@ -733,8 +769,8 @@ __device__ __forceinline__ void fp_group_sum(const RayGeom &r, const Geom &g,
     if (!fast) {
 #pragma unroll 1
         for (int q = 0; q < G; q++)
-            fp_slab<K, ONES, VT, CHECK>(r, g, sm_c[j + q][col], d0 + j + q, base, su, sd, sz, z_half,
-                                        zsafe, acc, accw);
+            fp_slab<K, ONES, VT, CHECK, PAIR>(r, g, sm_c[j + q][col], d0 + j + q, base, su, sd, sz,
+                                              z_half, zsafe, acc, accw);
         return;
     }
 #pragma unroll
@@ -784,7 +820,7 @@ __device__ __forceinline__ void fp_group_sum(const RayGeom &r, const Geom &g,
 // reference's order, so that a warp waits for memory once per group instead
 // of per slab.  A group whose footprints are not all 2x2 windows takes the
 // general per-slab path.
-template <int K, int G, bool ONES, typename VT, bool CHECK>
+template <int K, int G, bool ONES, typename VT, bool CHECK, bool PAIR = false>
 __device__ __forceinline__ void fp_chunk(const RayGeom &r, const Geom &g,
                                          const SlabC (*sm_c)[FPC_COLS], int col, int j0, int jend,
                                          int d0, const VT *const *base, int su, int sd, int sz,
@@ -793,14 +829,14 @@ __device__ __forceinline__ void fp_chunk(const RayGeom &r, const Geom &g,
     for (; j + G <= jend; j += G) {
         SlabZ w[G];
         float v[G][K][4];
-        const bool fast = fp_group_load<K, G, CHECK>(r, g, sm_c, col, j, sz, base, z_half,
-                                                  zsafe, w, v);
-        fp_group_sum<K, G, ONES, VT, CHECK>(r, g, sm_c, col, j, d0, base, su, sd, sz,
-                                         z_half, zsafe, fast, w, v, acc, accw);
+        const bool fast = fp_group_load<K, G, CHECK, VT, PAIR>(r, g, sm_c, col, j, sz, base,
+                                                            z_half, zsafe, w, v);
+        fp_group_sum<K, G, ONES, VT, CHECK, PAIR>(r, g, sm_c, col, j, d0, base, su, sd, sz,
+                                               z_half, zsafe, fast, w, v, acc, accw);
     }
     for (; j < jend; j++)
-        fp_slab<K, ONES, VT, CHECK>(r, g, sm_c[j][col], d0 + j, base, su, sd, sz, z_half, zsafe, acc,
-                                    accw);
+        fp_slab<K, ONES, VT, CHECK, PAIR>(r, g, sm_c[j][col], d0 + j, base, su, sd, sz, z_half,
+                                          zsafe, acc, accw);
 }
 
 // blockDim = FPC_THREADS: thread t is column t % FPC_COLS, row t / FPC_COLS;
@@ -837,8 +873,11 @@ constexpr int FPC_MIN_BLOCKS_K1 = 6;
 // MINB: resident blocks per SM the register budget must allow (the launch
 // shape the driver's tuning may choose, with G; every choice gives the same
 // bits).
+// PAIR (three volumes): the second and third volumes interleaved in one
+// array, vol.std[1] / vol.tr[1] (fp_voxel).
 template <int K, bool ONES, typename VT, typename MT = VT, bool MULTI = false,
-          int G = fp_group<K>(), int MINB = (K == 1 && G == 2) ? FPC_MIN_BLOCKS_K1 : FPC_MIN_BLOCKS>
+          int G = fp_group<K>(), int MINB = (K == 1 && G == 2) ? FPC_MIN_BLOCKS_K1 : FPC_MIN_BLOCKS,
+          bool PAIR = false>
 __global__ void __launch_bounds__(FPC_THREADS, MINB) fp_ref_kernel(const FPArgs<VT, K, MT> p) {
     __shared__ SlabC sm_c[FPC_CHUNK][FPC_COLS];
     __shared__ double2 sm_norm[FPC_THREADS / 32];
@@ -942,11 +981,11 @@ __global__ void __launch_bounds__(FPC_THREADS, MINB) fp_ref_kernel(const FPArgs<
         const int j0 = wlo <= whi ? max(sm_ur[0], wlo - d0) : 0;
         const int jend = (active && wlo <= whi) ? min(min(sm_ur[1], whi - d0) + 1, r.nd - d0) : 0;
         if (warp_exact)
-            fp_chunk<K, G, ONES, VT, false>(r, g, sm_c, col, max(j0, 0), jend, d0, base, su, sd,
-                                         sz, z_half, ax.zsafe, acc, accw);
+            fp_chunk<K, G, ONES, VT, false, PAIR>(r, g, sm_c, col, max(j0, 0), jend, d0, base, su,
+                                               sd, sz, z_half, ax.zsafe, acc, accw);
         else
-            fp_chunk<K, G, ONES, VT, true>(r, g, sm_c, col, max(j0, 0), jend, d0, base, su, sd, sz,
-                                        z_half, ax.zsafe, acc, accw);
+            fp_chunk<K, G, ONES, VT, true, PAIR>(r, g, sm_c, col, max(j0, 0), jend, d0, base, su,
+                                              sd, sz, z_half, ax.zsafe, acc, accw);
         __syncthreads();
     }
 

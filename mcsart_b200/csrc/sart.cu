@@ -120,8 +120,10 @@ template <typename ST, int INTERP, int SUM> struct Runner {
         MC_TRY(S.img1T.ensure(vs * subset));
         MC_TRY(S.imgS.ensure(vs));
         MC_TRY(S.imgST.ensure(vs));
-        MC_TRY(S.img0.ensure(vs));
-        MC_TRY(S.img0T.ensure(vs));
+        // img0 and the initial2 volume interleaved for the reference-order
+        // projector (PAIR), separate for the split-sum one
+        MC_TRY(S.img0.ensure(2 * vs));
+        MC_TRY(S.img0T.ensure(2 * vs));
         MC_TRY(S.ones.ensure(vs));
         MC_TRY(S.onesT.ensure(vs));
         MC_TRY(S.ratio.ensure(vf * subset));
@@ -179,7 +181,7 @@ template <typename ST, int INTERP, int SUM> struct Runner {
             a.bpcolA = S.bpcolA.as<float4>();
             a.bpcolB = S.bpcolB.as<float>();
         }
-        if (SUM == SUM_REF && K == 1) {
+        if constexpr (SUM == SUM_REF && K == 1) {
             // built-in: deeper slab groups when every block is resident at once
             const int var = tune.fp1 >= 0 ? tune.fp1 : fp_one_wave(ctx, fp_bx, fp_by) ? 1 : 0;
             // (slab-group depth, resident blocks per SM)
@@ -195,15 +197,16 @@ template <typename ST, int INTERP, int SUM> struct Runner {
                 default: MC_LAUNCH(ctx, (fp_ref_kernel<K, ONES, VT, ST, false, 2, 6>), grid,
                                    dim3(FPC_THREADS), 0, a);
             }
-        } else if (SUM == SUM_REF) {
+        } else if constexpr (SUM == SUM_REF) {
+            // three volumes, the second and third paired (enqueue_motion)
             switch (tune.fp3) {
-                case 1: MC_LAUNCH(ctx, (fp_ref_kernel<K, ONES, VT, ST, false, 2, 4>), grid,
+                case 1: MC_LAUNCH(ctx, (fp_ref_kernel<K, ONES, VT, ST, false, 2, 4, K == 3>), grid,
                                   dim3(FPC_THREADS), 0, a); break;
-                case 2: MC_LAUNCH(ctx, (fp_ref_kernel<K, ONES, VT, ST, false, 2, 5>), grid,
+                case 2: MC_LAUNCH(ctx, (fp_ref_kernel<K, ONES, VT, ST, false, 2, 5, K == 3>), grid,
                                   dim3(FPC_THREADS), 0, a); break;
-                case 3: MC_LAUNCH(ctx, (fp_ref_kernel<K, ONES, VT, ST, false, 4, 5>), grid,
+                case 3: MC_LAUNCH(ctx, (fp_ref_kernel<K, ONES, VT, ST, false, 4, 5, K == 3>), grid,
                                   dim3(FPC_THREADS), 0, a); break;
-                default: MC_LAUNCH(ctx, (fp_ref_kernel<K, ONES, VT, ST, false, 4, 4>), grid,
+                default: MC_LAUNCH(ctx, (fp_ref_kernel<K, ONES, VT, ST, false, 4, 4, K == 3>), grid,
                                    dim3(FPC_THREADS), 0, a);
             }
         } else if (opt.geom64) {
@@ -537,10 +540,15 @@ template <typename ST, int INTERP, int SUM> struct Runner {
         MC_LAUNCH(ctx, (transpose_kernel<float, ST>), tile_grid(), dim3(32, 8), 0,
                   S.imgST.as<ST>(), (const float *)P.img, g.nx, g.ny);
         vol.tr[0] = S.imgST.as<ST>();
+        // the reference-order projector reads img0 and the initial2 volume
+        // as interleaved pairs (one load for both), the split-sum one apart
+        constexpr bool pair = SUM == SUM_REF;
         vol.std[1] = S.img0.as<ST>();
         vol.tr[1] = S.img0T.as<ST>();
-        vol.std[2] = S.ones.as<ST>();
-        vol.tr[2] = S.onesT.as<ST>();
+        vol.std[2] = pair ? nullptr : S.ones.as<ST>();
+        vol.tr[2] = pair ? nullptr : S.onesT.as<ST>();
+        ST *const ones_std = pair ? nullptr : S.ones.as<ST>();
+        ST *const ones_tr = pair ? nullptr : S.onesT.as<ST>();
         // square slices: each view's field update and the next view's prep
         // run as one kernel (one pass over the fields)
         const bool fuse = g.nx == g.ny;
@@ -551,10 +559,10 @@ template <typename ST, int INTERP, int SUM> struct Runner {
             const float fd = P.flows[v] - P.flows[v - 1];
             if (!fuse || k == 0) {
                 ctx->label = "motion_prep";
-                MC_LAUNCH(ctx, (motion_prep_kernel<ST, ST>), tile_grid(), dim3(32, 8), 0,
-                          std_or_null(v, S.img0), tr_or_null(v, S.img0T), std_or_null(v, S.ones),
-                          tr_or_null(v, S.onesT), (const float *)P.img, f, g.nx, g.ny, g.nz, vd,
-                          fd);
+                MC_LAUNCH(ctx, (motion_prep_kernel<ST, ST, pair>), tile_grid(), dim3(32, 8), 0,
+                          std_or_null(v, S.img0), tr_or_null(v, S.img0T),
+                          reads_std[v] ? ones_std : nullptr, reads_tr[v] ? ones_tr : nullptr,
+                          (const float *)P.img, f, g.nx, g.ny, g.nz, vd, fd);
             }
             MC_TRY((launch_fp<3, false, ST>(vol, v, k, FP_MOTION)));
             MC_TRY(launch_bp(v, BP_DIV, S.ratio.as<float>(), nullptr));
@@ -565,20 +573,20 @@ template <typename ST, int INTERP, int SUM> struct Runner {
                 const float vdn = P.volumes[vn] - P.volumes[vn - 1];
                 const float fdn = P.flows[vn] - P.flows[vn - 1];
                 ctx->label = "field_update_prep";
+                ST *const o_std = reads_std[vn] ? ones_std : nullptr;
+                ST *const o_tr = reads_tr[vn] ? ones_tr : nullptr;
                 if (tune.fup == 1)
-                    MC_LAUNCH(ctx, (field_update_prep_kernel<ST, ST, true>), tile_grid(),
+                    MC_LAUNCH(ctx, (field_update_prep_kernel<ST, ST, true, pair>), tile_grid(),
                               dim3(32, 8), 0, fw, fw + V, fw + 2 * V, fw + 3 * V, fw + 4 * V,
                               fw + 5 * V, (const float *)S.ratio.as<float>(), (const float *)P.img,
                               g.nx, g.ny, g.nz, nvd, nfd, std_or_null(vn, S.img0),
-                              tr_or_null(vn, S.img0T), std_or_null(vn, S.ones),
-                              tr_or_null(vn, S.onesT), vdn, fdn);
+                              tr_or_null(vn, S.img0T), o_std, o_tr, vdn, fdn);
                 else
-                    MC_LAUNCH(ctx, (field_update_prep_kernel<ST, ST>), tile_grid(), dim3(32, 8),
-                              0, fw, fw + V, fw + 2 * V, fw + 3 * V, fw + 4 * V, fw + 5 * V,
-                              (const float *)S.ratio.as<float>(), (const float *)P.img, g.nx,
-                              g.ny, g.nz, nvd, nfd, std_or_null(vn, S.img0),
-                              tr_or_null(vn, S.img0T), std_or_null(vn, S.ones),
-                              tr_or_null(vn, S.onesT), vdn, fdn);
+                    MC_LAUNCH(ctx, (field_update_prep_kernel<ST, ST, false, pair>), tile_grid(),
+                              dim3(32, 8), 0, fw, fw + V, fw + 2 * V, fw + 3 * V, fw + 4 * V,
+                              fw + 5 * V, (const float *)S.ratio.as<float>(), (const float *)P.img,
+                              g.nx, g.ny, g.nz, nvd, nfd, std_or_null(vn, S.img0),
+                              tr_or_null(vn, S.img0T), o_std, o_tr, vdn, fdn);
             } else {
                 ctx->label = "field_update";
                 MC_LAUNCH(ctx, (field_update_kernel<ST>), tile_grid(), dim3(32, 8), 0, fw, fw + V,
