@@ -8,6 +8,8 @@ reference's own kernels and loop, rebuilt from its sources, bit for bit:
   of host_AUMISART overload 1;
 * the motion-compensated 256x256x160 workload (detector 512x384, 660 views):
   projector, backprojector and warp, and one outer iteration of the loop;
+  the 128x128x96 workload (detector 256x192, 360 views): one outer
+  iteration of the loop;
 * the clinical 512x512x256 size (detector 1024x768): projector,
   backprojector and warp, whose 256 MiB volume no longer fits the 126 MB L2,
   plus a size-independent property: a ray that stays inside the volume
@@ -82,15 +84,17 @@ def test_warp_matches_the_reference_at_config_3(ctx, torch_cuda, ref, c3):
     np.testing.assert_array_equal(host(out), ref.deform(img, 0.7, -0.3, F))
 
 
-def test_motion_loop_matches_the_reference_at_config_3(ctx, torch_cuda):
-    """The whole host_AUMISART loop at config 3's size (256x256x160 at 1 mm,
-    detector 512x384, 660 views, breathing motion; the benchmark's seeded
-    problem): one outer iteration, an image pass and a DVF-update pass,
+@pytest.mark.parametrize("cfg", ["c2", "c3"])
+def test_motion_loop_matches_the_reference_at_config_3(ctx, torch_cuda, cfg):
+    """The whole host_AUMISART loop at the motion workloads' full sizes
+    (256x256x160 at 1 mm with a 512x384 detector and 660 views, the
+    benchmark's seeded problem; 128x128x96 at 2 mm with 256x192 and 360
+    views): one outer iteration, an image pass and a DVF-update pass,
     against the reference's own loop rebuilt from its sources.  Volume,
     alpha_x and every residual projection agree bit for bit."""
     import bench
     from oracle import ref_runner
-    p, proj, fields = bench.build_problem(ctx, torch_cuda, "c3")
+    p, proj, fields = bench.build_problem(ctx, torch_cuda, cfg)
     g, nv = p.geo, p.cfg.n_views
     proj_h = np.ascontiguousarray(proj.cpu().numpy())
     F = [np.ascontiguousarray(f.cpu().numpy()) for f in fields]
