@@ -85,7 +85,7 @@ def test_warp_matches_the_reference_at_config_3(ctx, torch_cuda, ref, c3):
 
 
 @pytest.mark.parametrize("cfg", ["c2", "c3"])
-def test_motion_loop_matches_the_reference_at_config_3(ctx, torch_cuda, cfg):
+def test_motion_loop_matches_the_reference_at_full_size(ctx, torch_cuda, cfg):
     """The whole host_AUMISART loop at the motion workloads' full sizes
     (256x256x160 at 1 mm with a 512x384 detector and 660 views, the
     benchmark's seeded problem; 128x128x96 at 2 mm with 256x192 and 360
