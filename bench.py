@@ -1,13 +1,13 @@
 """Benchmark of the McSART engine: SART iterations/s on one or more B200s.
 
-Workload (default, --config c3): the motion-compensated McSART problem of
+Workload (default, --config motion256): the motion-compensated McSART problem of
 volume 256x256x160 at 1 mm, flat detector 512x384 at 0.776 mm, SAD/SDD
 1000/1500 mm, 660 views over 360 degrees at 15 views/s with a 5DCT breathing
 model.  One step is one outer iteration = one image-update pass over all 660
 views (warp, project, residual, backproject, normalise, inverse warp, update)
 plus one DVF-update pass over 659 views, i.e. host_AUMISART with op_iter =
-[1, 0].  --config c2 selects the 128x128x96 problem (detector 256x192 at
-1.2 mm, 360 views), c1 the static 64^3 one (60 views).  Inputs are seeded
+[1, 0].  --config motion128 selects the 128x128x96 problem (detector 256x192 at
+1.2 mm, 360 views), static64 the static 64^3 one (60 views).  Inputs are seeded
 synthetic data of that shape (phantom, smooth random DVF, projections of the
 warped phantom), generated outside the timed region.
 
@@ -46,7 +46,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
-    ap.add_argument("--config", default="c3")
+    ap.add_argument("--config", default="motion256")
     ap.add_argument("--cpu-views", type=int, default=0,
                     help="views per pass in the CPU sample (0 = auto)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -179,20 +179,20 @@ def algorithmic_bytes(p) -> dict:
 # step (cold cache, FP32 storage, built-in launch shapes); summaries with the
 # commands are kept under profiles/.
 NCU_DRAM_BYTES = {
-    "c3": {"fp_motion": 132488704, "fp_image": 42956032, "bp_div": 2872064,
+    "motion256": {"fp_motion": 132488704, "fp_image": 42956032, "bp_div": 2872064,
            "field_update_prep": 613819647},
 }
 
 # Issue-slot utilisation (smsp__issue_active) of the projector and
 # backprojector from the same captures: these kernels are bound by issue and
 # latency, not by HBM.
-NCU_ISSUE_ACTIVE = {"c3": {"fp_image": 0.570, "fp_motion": 0.606, "bp_div": 0.803}}
+NCU_ISSUE_ACTIVE = {"motion256": {"fp_image": 0.570, "fp_motion": 0.606, "bp_div": 0.803}}
 
 # Views per pass of the CPU samples: the engine line's cpu_baseline leg
 # (about 10 s of CPU work) and each step of the reference arm (a few seconds,
 # so that --steps 20 --warmup 5 ends within a few minutes).
-CPU_VIEWS = {"c1": 60, "c2": 160, "c3": 16, "c5": 4}
-REF_ARM_VIEWS = {"c1": 30, "c2": 64, "c3": 6, "c5": 2}
+CPU_VIEWS = {"static64": 60, "motion128": 160, "motion256": 16, "clinical512": 4}
+REF_ARM_VIEWS = {"static64": 30, "motion128": 64, "motion256": 6, "clinical512": 2}
 
 
 def measured_peaks() -> dict:
@@ -401,7 +401,7 @@ def run_kernel_case(args, ctx, torch, stream):
 
 
 def run_batch_config(args, ctx, torch, stream, m, rank, world):
-    """--config c4: the 8 seeded uneven problems (96x96x64 .. 256x256x128,
+    """--config batch8: the 8 seeded uneven problems (96x96x64 .. 256x256x128,
     detectors 192x128 .. 512x384, 120 .. 660 views) reconstructed together by
     mcsart_batch_run, image passes in ordered subsets of 10 views.  One step =
     one outer iteration (image pass + DVF-update pass) of every problem.
@@ -460,7 +460,7 @@ def run_batch_config(args, ctx, torch, stream, m, rank, world):
             "warmup": args.warmup, "ms_per_step": 1000.0 * len(probs) / out["f32"]["batch"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
-            "config": {"workload": "c4: 8 uneven motion-compensated problems, one outer "
+            "config": {"workload": "batch8: 8 uneven motion-compensated problems, one outer "
                                    "iteration each per step, ordered subsets of 10 views",
                        "problems": [c.name for c in cfgs],
                        "l2": "flushed before every timed step (256 MiB write)"},
@@ -501,7 +501,7 @@ def main():
         if dist_on:
             dist.destroy_process_group()
         return
-    if args.config == "c4":
+    if args.config == "batch8":
         run_batch_config(args, ctx, torch, stream, m, rank, world)
         ctx.close()
         if dist_on:

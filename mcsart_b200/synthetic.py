@@ -1,16 +1,16 @@
 """Seeded synthetic McSART problems: phantom, cone-beam geometry, 5DCT motion.
 
-The workloads follow the benchmark configurations of the McSART engine:
+The workloads (keys of CONFIGS; the batch is ``batch_configs``):
 
-  config 1: static SART, 64^3 at 2 mm, detector 128x96 at 1.6 mm, 60 views, 5 iterations
-  config 2: motion-compensated, 128x128x96 at 2 mm, 256x192 at 1.2 mm, 360 views,
-            10 outer iterations of SART + DVF update
-  config 3: motion-compensated, 256x256x160 at 1 mm, 512x384 at 0.776 mm, 660 views
-  config 4: 8 independent motion-compensated problems of seeded uneven sizes
-            (volumes 96x96x64 to 256x256x128 at 1-2 mm, detectors 192x128 to
-            512x384, 120-660 views each), reconstructed together in ordered
-            subsets of 10 views (``batch_configs``)
-  config 5: 512x512x256 at 0.5 mm, 1024x768 at 0.388 mm, 1320 views
+  static64:    static SART, 64^3 at 2 mm, detector 128x96 at 1.6 mm, 60 views, 5 iterations
+  motion128:   motion-compensated, 128x128x96 at 2 mm, 256x192 at 1.2 mm, 360 views,
+               10 outer iterations of SART + DVF update
+  motion256:   motion-compensated, 256x256x160 at 1 mm, 512x384 at 0.776 mm, 660 views
+  batch8:      8 independent motion-compensated problems of seeded uneven
+               sizes (volumes 96x96x64 to 256x256x128 at 1-2 mm, detectors
+               192x128 to 512x384, 120-660 views each), reconstructed together
+               in ordered subsets of 10 views (``batch_configs``)
+  clinical512: 512x512x256 at 0.5 mm, 1024x768 at 0.388 mm, 1320 views
 
 Phantom: 10 ellipsoids with centres uniform in a 50 mm ball, semi-axes U[5, 40] mm,
 random rotation, attenuation U[0, 0.04]/mm, added together; motion configs add a
@@ -51,12 +51,12 @@ class Config:
 
 
 CONFIGS = {
-    "c1": Config("static SART 64^3, 60 views", 64, 64, 64, 2.0, 128, 96, 1.6, 60, 5, False, False),
-    "c2": Config("motion-compensated McSART 128x128x96, 360 views", 128, 128, 96, 2.0, 256, 192,
+    "static64": Config("static SART 64^3, 60 views", 64, 64, 64, 2.0, 128, 96, 1.6, 60, 5, False, False),
+    "motion128": Config("motion-compensated McSART 128x128x96, 360 views", 128, 128, 96, 2.0, 256, 192,
                  1.2, 360, 10, True, True),
-    "c3": Config("motion-compensated McSART 256x256x160, 660 views", 256, 256, 160, 1.0, 512, 384,
+    "motion256": Config("motion-compensated McSART 256x256x160, 660 views", 256, 256, 160, 1.0, 512, 384,
                  0.776, 660, 10, True, True),
-    "c5": Config("clinical McSART 512x512x256, 1320 views", 512, 512, 256, 0.5, 1024, 768, 0.388,
+    "clinical512": Config("clinical McSART 512x512x256, 1320 views", 512, 512, 256, 0.5, 1024, 768, 0.388,
                  1320, 10, True, True, si_mm=15.0, aplr_mm=4.5),
 }
 
@@ -70,7 +70,7 @@ BATCH_SUBSET = 10
 
 
 def batch_configs(n: int = 8, seed: int = 0) -> list[Config]:
-    """The uneven batch of config 4: n motion-compensated problems of seeded
+    """The uneven batch (batch8): n motion-compensated problems of seeded
     sizes.  The first two are the extremes (96x96x64 with a 192x128 detector
     and 120 views; 256x256x128 with 512x384 and 660 views), the others drawn
     from the size sets above; views are multiples of the subset size 10 in

@@ -89,10 +89,10 @@ def test_synthetic_problem_is_seeded_and_shaped():
 
 
 def test_synthetic_geometry_matches_the_benchmark_configs():
-    g = S.geometry(S.CONFIGS["c1"])
+    g = S.geometry(S.CONFIGS["static64"])
     assert (g["SO"], g["SD"], g["da"]) == (500.0, 750.0, pytest.approx(0.8))
     assert g["ai"] == -63.5 and g["bi"] == -47.5
-    g2 = S.geometry(S.CONFIGS["c2"])
+    g2 = S.geometry(S.CONFIGS["motion128"])
     assert (g2["nx"], g2["nz"], g2["na"], g2["nb"]) == (128, 96, 256, 192)
     assert g2["da"] == pytest.approx(0.6)
 

@@ -47,16 +47,16 @@ def _smooth_volume(shape, seed):
 
 
 @pytest.fixture(scope="module")
-def c3():
-    g = _geo("c3")
+def motion256():
+    g = _geo("motion256")
     return g, _smooth_volume((g["nz"], g["ny"], g["nx"]), 31)
 
 
 @pytest.mark.parametrize("angle", [0.3, 0.7853982, 2.4, 4.0])
-def test_projection_and_backprojection_match_the_reference_at_config_3(ctx, torch_cuda, ref, c3,
+def test_projection_and_backprojection_match_the_reference_at_256x256x160(ctx, torch_cuda, ref, motion256,
                                                                       angle):
     torch = torch_cuda
-    g, img = c3
+    g, img = motion256
     args = (g["SO"], g["SD"], g["da"], g["na"], g["ai"], g["db"], g["nb"], g["bi"], g["nx"],
             g["ny"], g["nz"])
     d_img = dev(torch, img)
@@ -72,9 +72,9 @@ def test_projection_and_backprojection_match_the_reference_at_config_3(ctx, torc
     np.testing.assert_array_equal(host(d_bp), ref.backprojection(mine, angle, g))
 
 
-def test_warp_matches_the_reference_at_config_3(ctx, torch_cuda, ref, c3):
+def test_warp_matches_the_reference_at_256x256x160(ctx, torch_cuda, ref, motion256):
     torch = torch_cuda
-    g, img = c3
+    g, img = motion256
     shape = img.shape
     F = [(_smooth_volume(shape, 40 + c) - np.float32(0.5)) * np.float32(4) for c in range(6)]
     out = torch.empty_like(dev(torch, img))
@@ -84,7 +84,7 @@ def test_warp_matches_the_reference_at_config_3(ctx, torch_cuda, ref, c3):
     np.testing.assert_array_equal(host(out), ref.deform(img, 0.7, -0.3, F))
 
 
-@pytest.mark.parametrize("cfg", ["c2", "c3"])
+@pytest.mark.parametrize("cfg", ["motion128", "motion256"])
 def test_motion_loop_matches_the_reference_at_full_size(ctx, torch_cuda, cfg):
     """The whole host_AUMISART loop at the motion workloads' full sizes
     (256x256x160 at 1 mm with a 512x384 detector and 660 views, the
@@ -115,7 +115,7 @@ def test_motion_loop_matches_the_reference_at_full_size(ctx, torch_cuda, cfg):
     np.testing.assert_array_equal(out["resid"], r["resid"])
 
 
-def test_static_loop_matches_the_reference_at_config_1(ctx, torch_cuda, ref):
+def test_static_loop_matches_the_reference_at_64_cubed(ctx, torch_cuda, ref):
     """host_AUMISART overload 1 at the static workload's size (64x64x64 at 2 mm,
     detector 128x96, 60 views, 5 image passes), the measured projections made
     by the reference's own projector: volume and residuals bit for bit the
@@ -123,7 +123,7 @@ def test_static_loop_matches_the_reference_at_config_1(ctx, torch_cuda, ref):
     from mcsart_b200 import synthetic as S
     from oracle import ref_runner
     from conftest import rel_l2
-    p = S.make_problem("c1", 0)
+    p = S.make_problem("static64", 0)
     g, nv = p.geo, p.cfg.n_views
     proj = ref.motion_projections(p.truth, None, p.volumes, p.flows, p.angles, g)
     op = np.ones(5, np.int32)
@@ -145,18 +145,18 @@ def test_static_loop_matches_the_reference_at_config_1(ctx, torch_cuda, ref):
 
 
 @pytest.fixture(scope="module")
-def c5():
-    g = _geo("c5")
+def clinical512():
+    g = _geo("clinical512")
     return g, _smooth_volume((g["nz"], g["ny"], g["nx"]), 51)
 
 
 @pytest.mark.parametrize("angle", [0.3, 0.7853982, 2.4])
-def test_projection_and_backprojection_match_the_reference_at_config_5(ctx, torch_cuda, ref, c5,
+def test_projection_and_backprojection_match_the_reference_at_512x512x256(ctx, torch_cuda, ref, clinical512,
                                                                       angle):
     """512x512x256 volume, 1024x768 detector: both driving axes and the
     45-degree switch, bit for bit the reference's kernels."""
     torch = torch_cuda
-    g, img = c5
+    g, img = clinical512
     d_img = dev(torch, img)
     d_proj = torch.empty((g["nb"], g["na"]), device="cuda")
     ctx.host_projection(d_proj, d_img, angle, *_args(g))
@@ -170,9 +170,9 @@ def test_projection_and_backprojection_match_the_reference_at_config_5(ctx, torc
     del d_img, d_bp
 
 
-def test_warp_matches_the_reference_at_config_5(ctx, torch_cuda, ref, c5):
+def test_warp_matches_the_reference_at_512x512x256(ctx, torch_cuda, ref, clinical512):
     torch = torch_cuda
-    g, img = c5
+    g, img = clinical512
     shape = img.shape
     F = [(_smooth_volume(shape, 60 + c) - np.float32(0.5)) * np.float32(6) for c in range(6)]
     d_img = dev(torch, img)
@@ -182,7 +182,7 @@ def test_warp_matches_the_reference_at_config_5(ctx, torch_cuda, ref, c5):
     np.testing.assert_array_equal(host(out), ref.deform(img, -0.9, 0.4, F))
 
 
-def test_uneven_batch_matches_separate_runs_at_config_4(ctx, torch_cuda):
+def test_uneven_batch_matches_separate_runs(ctx, torch_cuda):
     """The 8 seeded problems of the uneven batch (96x96x64 .. 256x256x128,
     detectors 192x128 .. 512x384, 120 .. 660 views), one outer iteration
     (image pass in ordered subsets of 10 views, then the DVF pass) through
@@ -225,9 +225,9 @@ def test_uneven_batch_matches_separate_runs_at_config_4(ctx, torch_cuda):
         assert np.isfinite(alone[i]["img"]).all()
 
 
-def test_central_rays_count_slabs_at_config_5(ctx, torch_cuda):
+def test_central_rays_count_slabs_at_512x512x256(ctx, torch_cuda):
     torch = torch_cuda
-    g = _geo("c5")
+    g = _geo("clinical512")
     ones = torch.ones((g["nz"], g["ny"], g["nx"]), device="cuda")
     d_proj = torch.empty((g["nb"], g["na"]), device="cuda")
     ctx.host_projection(d_proj, ones, 0.0, g["SO"], g["SD"], g["da"], g["na"], g["ai"], g["db"],

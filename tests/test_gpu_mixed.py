@@ -53,17 +53,17 @@ def _args(g):
 
 
 @pytest.fixture(scope="module")
-def c3_problem(ctx, torch_cuda):
+def motion256_problem(ctx, torch_cuda):
     """The seeded 256x256x160 problem (phantom, DVF), inputs at BF16 precision."""
     from mcsart_b200 import synthetic as S
     torch = torch_cuda
-    p = S.make_problem("c3", 0)
+    p = S.make_problem("motion256", 0)
     truth = _bf16(torch, p.truth)
     F = [_bf16(torch, f) for f in p.fields]
     return p, truth, F
 
 
-def test_kernel_errors_vs_fp64_oracle_at_config_3_size(ctx, torch_cuda, oracle, c3_problem):
+def test_kernel_errors_vs_fp64_oracle_at_256x256x160(ctx, torch_cuda, oracle, motion256_problem):
     """One call of each kernel form against the FP64 oracle of the same
     inputs.  Bounds: FP32-storage forms within 1e-5 relative L2; forms whose
     input or output is stored in 16 bits within that type's unit roundoff
@@ -71,7 +71,7 @@ def test_kernel_errors_vs_fp64_oracle_at_config_3_size(ctx, torch_cuda, oracle, 
     weights) within 1e-2."""
     import mcsart_b200 as m
     torch = torch_cuda
-    p, truth, F = c3_problem
+    p, truth, F = motion256_problem
     g = p.geo
     angle = 0.3  # x-driven rays
     o_fp = oracle.projection(truth, angle, g)
@@ -122,8 +122,8 @@ def test_kernel_errors_vs_fp64_oracle_at_config_3_size(ctx, torch_cuda, oracle, 
         assert e <= tol, (name, e)
 
 
-def test_volume_error_after_10_image_passes_at_config_3_size(ctx, torch_cuda, oracle,
-                                                              c3_problem):
+def test_volume_error_after_10_image_passes_at_256x256x160(ctx, torch_cuda, oracle,
+                                                              motion256_problem):
     """Motion-compensated SART with the DVF held fixed (10 image passes; the
     DVF-update pass divides by a signed normaliser and so amplifies any
     rounding difference without bound, see test_golden_shows_the_dvf_update_
@@ -133,7 +133,7 @@ def test_volume_error_after_10_image_passes_at_config_3_size(ctx, torch_cuda, or
     relative L2 of the FP64 oracle."""
     import mcsart_b200 as m
     torch = torch_cuda
-    p, truth, F = c3_problem
+    p, truth, F = motion256_problem
     g = p.geo
     sel = np.arange(0, p.cfg.n_views, 55)
     nv = len(sel)
