@@ -179,14 +179,14 @@ def algorithmic_bytes(p) -> dict:
 # step (cold cache, FP32 storage, built-in launch shapes); summaries with the
 # commands are kept under profiles/.
 NCU_DRAM_BYTES = {
-    "motion256": {"fp_motion": 132488704, "fp_image": 42956032, "bp_div": 2872064,
+    "motion256": {"fp_motion": 132078080, "fp_image": 42956032, "bp_div": 2872064,
            "field_update_prep": 613819647},
 }
 
 # Issue-slot utilisation (smsp__issue_active) of the projector and
 # backprojector from the same captures: these kernels are bound by issue and
 # latency, not by HBM.
-NCU_ISSUE_ACTIVE = {"motion256": {"fp_image": 0.570, "fp_motion": 0.606, "bp_div": 0.803}}
+NCU_ISSUE_ACTIVE = {"motion256": {"fp_image": 0.570, "fp_motion": 0.602, "bp_div": 0.803}}
 
 # Views per pass of the CPU samples: the engine line's cpu_baseline leg
 # (about 10 s of CPU work) and each step of the reference arm (a few seconds,

@@ -170,17 +170,22 @@ def test_graph_cache_tells_bf16_from_f16_on_the_same_buffers(ctx, torch_cuda, or
         np.testing.assert_array_equal(run(s, 1), direct[s])
 
 
-@pytest.mark.parametrize("storage,tol", [(0, 2e-5), (1, 1e-2), (2, 2e-3)])
+@pytest.mark.parametrize("storage,tol", [(0, 2e-5), (1, 1e-3), (2, 1e-3)])
 def test_mixed_precision_error_vs_fp64_oracle(ctx, torch_cuda, oracle, storage, tol):
     """Motion-compensated SART (5 image passes, fixed DVF) with FP32/BF16/FP16
     storage of the DVF fields, warped volumes and projections and FP32
-    arithmetic, against the FP64 oracle with exact trilinear weights.  (The
-    DVF-update pass is left out: its division by a signed normaliser makes any
-    two implementations diverge, see test_golden_shows_the_dvf_update...)"""
+    arithmetic, against the FP64 oracle with exact trilinear weights.  The
+    measured projections and the fields are given at the storage type's
+    precision to both, so the error is the engine's intermediate storage and
+    arithmetic, not the rounding of its inputs.  (The DVF-update pass is left
+    out: its division by a signed normaliser makes any two implementations
+    diverge, see test_golden_shows_the_dvf_update...)"""
     import mcsart_b200 as m
     torch = torch_cuda
     dt = {0: torch.float32, 1: torch.bfloat16, 2: torch.float16}[storage]
     g, it, img0, proj, F = make_case(oracle, motion=True, seed=11, op_iter=(1, 1, 1, 1, 1))
+    proj = torch.as_tensor(proj).to(dt).float().numpy()
+    F = [torch.as_tensor(f).to(dt).float().numpy() for f in F]
     o = oracle.aumisart(img0, proj, g, it, F, tex_mode=oracle.TEX_EXACT)
     d_img = dev(torch, img0)
     d_proj = dev(torch, proj).to(dt)
