@@ -55,6 +55,9 @@ def parse():
     ap.add_argument("--profile-steps", type=int, default=0,
                     help="only run this many untimed steps inside the NVTX range "
                          "'mcsart_step' (for a profiler's launch list) and exit")
+    ap.add_argument("--profile-subset", type=int, default=1,
+                    help="with --profile-steps: image passes in ordered subsets of this many "
+                         "views (not the drop-in; 1 = the reference's view-by-view loop)")
     ap.add_argument("--no-autotune", action="store_true",
                     help="run the driver with its built-in launch shapes instead of tuning "
                          "them for the workload in the warm-up (mcsart_autotune)")
@@ -551,9 +554,11 @@ def main():
     # for the workload on the first (warm-up) run, which changes no result bit
     drop_in = m.default_options(autotune=0 if args.no_autotune else 1)
     if args.profile_steps:
+        prof_opt = (drop_in if args.profile_subset <= 1 else
+                    m.default_options(autotune=drop_in.autotune, subset=args.profile_subset))
         for _ in range(args.profile_steps):
             torch.cuda.nvtx.range_push("mcsart_step")
-            step(drop_in, img, F)
+            step(prof_opt, img, F)
             torch.cuda.nvtx.range_pop()
         torch.cuda.synchronize()
         if rank == 0:
