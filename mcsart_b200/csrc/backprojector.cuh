@@ -133,9 +133,9 @@ struct BPArgs {
     int n_views;
     const float *angles;
     cudaSurfaceObject_t outSurfs[16];
-    // single view: the view's column data (bp_column for every (ix, iy),
-    // index ix + iy*nx), computed by the projector launch before this one;
-    // nullptr = compute it here
+    // the views' column data (bp_column for every (ix, iy), index
+    // ix + iy*nx, view v of the launch at + v*nx*ny), computed by the
+    // projector launch before this one; nullptr = compute it here
     const float4 *colA;  // amin, amax, rl, rr
     const float *colB;   // r0
 };
@@ -165,12 +165,12 @@ constexpr int BP_WB = 4;
 template <int K, bool PROVEN, int NZ = BP_NZ>
 __device__ __forceinline__ void bp_gather_view(const BPArgs &p, float angle, const float *proj,
                                                const float2 *pair, int ix, int iy, int z0,
-                                               float *acc0, float *acc1) {
+                                               float *acc0, float *acc1, int view = 0) {
     const Geom &g = p.g;
     const int na = g.na;
     BPColumn col;
     if (p.colA != nullptr) {
-        const int64_t c = ix + (int64_t)iy * g.nx;
+        const int64_t c = ix + ((int64_t)iy + (int64_t)view * g.ny) * g.nx;
         const float4 a = __ldg(p.colA + c);
         col.amin = a.x;
         col.amax = a.y;
@@ -337,7 +337,7 @@ __global__ void __launch_bounds__(256, MCSART_BP_MINBLOCKS) bp_kernel(const BPAr
             if (active) bp_gather_view64<K, NZ>(p, angle, p.proj, p.pair, ix, iy, z0, acc0, acc64);
         } else if (active) {
             bp_gather_view<K, PROVEN, NZ>(p, angle, p.proj, p.pair + v * NP, ix, iy, z0, acc0,
-                                          acc1);
+                                          acc1, v);
         }
 #pragma unroll
         for (int k = 0; k < NZ; k++) {

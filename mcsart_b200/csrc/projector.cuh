@@ -380,9 +380,9 @@ template <typename VT, int K, typename MT = VT> struct FPArgs {
     // one view, and the volumes by vol_stride elements per view (0: every
     // view projects the same volumes)
     int64_t vol_stride;
-    // single view: when set, also write the view's backprojector column data
-    // (bp_column for every (ix, iy), index ix + iy*nx) for the backprojector
-    // launch that follows
+    // when set, also write each view's backprojector column data (bp_column
+    // for every (ix, iy), index ix + iy*nx, view j of a several-view launch at
+    // + j*nx*ny) for the backprojector launch that follows
     float4 *bpcolA;  // amin, amax, rl, rr
     float *bpcolB;   // r0
 };
@@ -989,19 +989,20 @@ __global__ void __launch_bounds__(FPC_THREADS, MINB) fp_ref_kernel(const FPArgs<
         __syncthreads();
     }
 
-    if (!MULTI && p.bpcolA != nullptr) {
+    if (p.bpcolA != nullptr) {
         // the following backprojector's per-column part, with its own sine
         // and cosine of the angle (src/cu_backprojection.cu:62-63): the same
         // device code, so the same bits as computing it there; spread over
-        // all threads of the launch
+        // all threads of the view's blocks
         const float bs = __sinf(angle), bc = __cosf(angle);
         const int64_t ncol = (int64_t)g.nx * g.ny;
+        const int64_t coff = MULTI ? (int64_t)blockIdx.z * ncol : 0;
         const int64_t nthr = (int64_t)gridDim.x * gridDim.y * FPC_THREADS;
         for (int64_t c = ((int64_t)blockIdx.y * gridDim.x + blockIdx.x) * FPC_THREADS + t; c < ncol;
              c += nthr) {
             const BPColumn col = bp_column<false>((int)(c % g.nx), (int)(c / g.nx), bc, bs, g);
-            p.bpcolA[c] = make_float4(col.amin, col.amax, col.rl, col.rr);
-            p.bpcolB[c] = col.r0;
+            p.bpcolA[coff + c] = make_float4(col.amin, col.amax, col.rl, col.rr);
+            p.bpcolB[coff + c] = col.r0;
         }
     }
 

@@ -73,7 +73,8 @@ template <typename ST, int INTERP, int SUM> struct Runner {
     int fp_bx = 0, fp_by = 0, fp_blocks = 0, groups = 1;
     int subset = 1;  // views per ordered subset in image passes
     int inv_iters = 0;  // fixed-point steps of the true DVF inverse (0: negated amplitudes)
-    int cols_view = -1;  // view whose backprojector column data the last projector wrote
+    int cols_view = -1;  // first view whose backprojector column data the last projector wrote
+    int cols_views = 0;  // and how many views from it
     std::vector<int> views_img, views_mot;
     std::vector<char> reads_std, reads_tr;  // per view: the copies its projector reads
     Tuning tune;  // launch shapes (variant indices; -1 = built-in choice)
@@ -129,8 +130,8 @@ template <typename ST, int INTERP, int SUM> struct Runner {
         MC_TRY(S.ratio.ensure(vf * subset));
         MC_TRY(S.imgT.ensure(vf));
         MC_TRY(S.pairs.ensure(NP * subset * sizeof(float2)));
-        MC_TRY(S.bpcolA.ensure((size_t)P.g.nx * P.g.ny * sizeof(float4)));
-        MC_TRY(S.bpcolB.ensure((size_t)P.g.nx * P.g.ny * sizeof(float)));
+        MC_TRY(S.bpcolA.ensure((size_t)P.g.nx * P.g.ny * subset * sizeof(float4)));
+        MC_TRY(S.bpcolB.ensure((size_t)P.g.nx * P.g.ny * subset * sizeof(float)));
         if (INTERP == MCSART_INTERP_TEXTURE && P.motion_model) {
             MC_TRY(S.tv_img.ensure(P.g.nx, P.g.ny, P.g.nz));
             MC_TRY(S.tv_ratio.ensure(P.g.nx, P.g.ny, P.g.nz));
@@ -177,6 +178,7 @@ template <typename ST, int INTERP, int SUM> struct Runner {
         // the reference-order projector also writes the column data of this
         // view's backprojector, which follows it
         cols_view = SUM == SUM_REF ? v : -1;
+        cols_views = 1;
         if (SUM == SUM_REF) {
             a.bpcolA = S.bpcolA.as<float4>();
             a.bpcolB = S.bpcolB.as<float>();
@@ -289,6 +291,11 @@ template <typename ST, int INTERP, int SUM> struct Runner {
         a.bp_in = S.pairs.as<float2>();
         a.norm_part = S.norm_part.as<double2>() + (int64_t)k0 * fp_blocks;
         a.vol_stride = vol_stride;
+        // the kk views' backprojector column data for the launch that follows
+        a.bpcolA = S.bpcolA.as<float4>();
+        a.bpcolB = S.bpcolB.as<float>();
+        cols_view = v0;
+        cols_views = kk;
         ctx->label = mode == FP_MOTION ? "fp_motion" : "fp_image";
         MC_LAUNCH(ctx, (fp_ref_kernel<K, ONES, VT, ST, true>), dim3(fp_bx, fp_by, kk),
                   dim3(FPC_THREADS), 0, a);
@@ -310,6 +317,10 @@ template <typename ST, int INTERP, int SUM> struct Runner {
         b.out = out;
         b.outT = outT;
         for (int j = 0; j < kk && surfs; j++) b.outSurfs[j] = surfs[j];
+        if (cols_view == v0 && cols_views == kk) {  // written by the subset's projector launch
+            b.colA = S.bpcolA.as<float4>();
+            b.colB = S.bpcolB.as<float>();
+        }
         const dim3 grid(div_up(P.g.nx, 32), div_up(P.g.ny, BP_ROWS), div_up(P.g.nz, BP_NZ)),
             block(32, BP_ROWS);
         const bool proven = bp_geom_proven(P.g);
