@@ -145,17 +145,25 @@ constexpr int BP_MAX_VIEWS = 16;
 #ifndef MCSART_BP_NZ
 #define MCSART_BP_NZ 2
 #endif
-#ifndef MCSART_BP_MINBLOCKS
-#define MCSART_BP_MINBLOCKS 1
-#endif
 // 4 rows: 128-thread blocks fill the SMs' slots in fewer partial waves than
 // 256-thread ones (9 resident per SM at 56 registers); 2.5 % less
 // backprojector time than 32 x 8 at both benchmark sizes.
 constexpr int BP_ROWS = 4;
 constexpr int BP_NZ = MCSART_BP_NZ;
 // Row weights kept in registers per slice; footprints taller than this many
-// detector rows take the general loop.
+// detector rows take the general loop (3 measured 12 % slower at 256x256x160:
+// about a fifth of the voxels need 4 rows there).
 constexpr int BP_WB = 4;
+// Resident 256-thread blocks per SM the register budget must allow (the
+// launch-bounds minimum): for the single-view kernel with FP32 geometry and
+// up to 2 voxels per thread 5, i.e. at most 48 registers, which it fits
+// without spilling (10 resident 128-thread blocks instead of 9 at 55
+// registers): backprojector time -1 % at 256x256x160; 6 (40 registers)
+// spills and was 3 % slower.  The several-view form (75 registers) was 5 %
+// slower per view under the same bound and keeps its own allocation.
+template <bool GEO64, bool MULTI, int NZ> constexpr int bp_min_blocks() {
+    return (!GEO64 && !MULTI && NZ <= 2) ? 5 : 1;
+}
 
 // Overlap-weighted gather of one view for the NZ voxels (ix, iy, z0 ..)
 // of a thread: acc0 (and acc1 with K == 2) get the view's terms in the
@@ -311,7 +319,7 @@ __device__ __forceinline__ void bp_gather_view64(const BPArgs &p, float angle, c
 // bits (each voxel's terms and their order do not depend on it).
 template <int K, int MODE, bool MULTI = false, bool PROVEN = false, bool GEO64 = false,
           int NZ = BP_NZ, int ROWS = BP_ROWS>
-__global__ void __launch_bounds__(256, MCSART_BP_MINBLOCKS) bp_kernel(const BPArgs p) {
+__global__ void __launch_bounds__(256, (bp_min_blocks<GEO64, MULTI, NZ>())) bp_kernel(const BPArgs p) {
     __shared__ float tile[NZ][ROWS][33];
     const Geom &g = p.g;
     const int tx = threadIdx.x, ty = threadIdx.y;
