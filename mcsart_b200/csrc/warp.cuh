@@ -123,6 +123,46 @@ static __global__ void __launch_bounds__(256) deform2_kernel(float *out, const f
     }
 }
 
+// L2 prefetch for the image pass's warp kernels.  Each voxel's six field
+// loads are followed by a dependent texture fetch, so at full occupancy the
+// kernels wait on load latency (ncu at 256x256x160: 26 long-scoreboard
+// stalls per issue, 4.5 TB/s).  Each block therefore prefetches into L2
+// (prefetch.global.L2, no registers, no result changes) the rows of the six
+// fields, and optionally of one more volume, that the block
+// WARP_PREFETCH_AHEAD blocks later in dispatch order (x fastest, then y, then
+// z) will read: one row segment of 32 voxels per thread.  600 blocks is about
+// half of those resident at once (8 per SM on 148 SMs); measured at
+// 256x256x160: warp_fwd 47.4 to 37.3 ms and warp_back_add 59.6 to 55.2 ms per
+// step (1200 blocks: 37.7 and 55.7).  The DVF pass's field update, which
+// also writes the fields, was slower with it (97.0 to 103.9 ms).
+constexpr int WARP_PREFETCH_AHEAD = 600;
+
+// The prefetch for a block of a grid of 32 x TH tiles (gridDim.x x gridDim.y
+// per slice, gridDim.z slices); t = the thread's index in the block.
+template <typename FT>
+__device__ __forceinline__ void prefetch_tile_rows(const Fields<FT> &f, const float *extra,
+                                                   int TH, int nx, int ny, int nz, int t) {
+    const int64_t gx = gridDim.x, gy = gridDim.y;
+    const int64_t b = blockIdx.x + gx * (blockIdx.y + gy * blockIdx.z) + WARP_PREFETCH_AHEAD;
+    const int arrays = extra ? 7 : 6;
+    if (t >= arrays * TH || b >= gx * gy * gridDim.z) return;
+    const int bx = (int)(b % gx), by = (int)((b / gx) % gy), bz = (int)(b / (gx * gy));
+    const int a = t / TH, y = by * TH + t % TH, x = bx * 32;
+    if (y >= ny || x >= nx || bz >= nz) return;
+    const int64_t i = x + (int64_t)y * nx + (int64_t)bz * nx * ny;
+    const void *p;
+    switch (a) {
+        case 0: p = f.ax + i; break;
+        case 1: p = f.ay + i; break;
+        case 2: p = f.az + i; break;
+        case 3: p = f.bx + i; break;
+        case 4: p = f.by + i; break;
+        case 5: p = f.bz + i; break;
+        default: p = extra + i;
+    }
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
 // Rows of voxels per thread in the image pass's warp kernels: a block covers
 // a 32 x (8 * WARP_ROWS) (x, y) tile of one slice.  2 measured best: 4 rows
 // leave a 128x128x96 volume's 1536 blocks in 1.3 waves (warp_fwd 11 % slower
@@ -148,6 +188,7 @@ static __global__ void __launch_bounds__(256) warp_fwd_kernel(VT *dst, VT *dstT,
     const int x0 = blockIdx.x * 32, y0 = blockIdx.y * TH, iz = blockIdx.z;
     const int64_t slice = (int64_t)iz * nx * ny;
     const int xm = x0 + tx;
+    prefetch_tile_rows(f, nullptr, TH, nx, ny, nz, ty * 32 + tx);
 #pragma unroll
     for (int k = 0; k < WR; k++) {
         const int ly = ty + 8 * k, ym = y0 + ly;
@@ -185,6 +226,7 @@ static __global__ void __launch_bounds__(256) warp_back_add_kernel(
     const int tx = threadIdx.x, ty = threadIdx.y;
     const int xm = blockIdx.x * 32 + tx, iz = blockIdx.z;
     const int64_t slice = (int64_t)iz * nx * ny;
+    prefetch_tile_rows(f, nullptr, 8 * WR, nx, ny, nz, ty * 32 + tx);
     if (xm >= nx) return;
 #pragma unroll
     for (int k = 0; k < WR; k++) {
