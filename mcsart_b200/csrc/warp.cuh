@@ -132,9 +132,11 @@ static __global__ void __launch_bounds__(256) deform2_kernel(float *out, const f
 // WARP_PREFETCH_AHEAD blocks later in dispatch order (x fastest, then y, then
 // z) will read: one row segment of 32 voxels per thread.  600 blocks is about
 // half of those resident at once (8 per SM on 148 SMs); measured at
-// 256x256x160: warp_fwd 47.4 to 37.3 ms and warp_back_add 59.6 to 55.2 ms per
-// step (1200 blocks: 37.7 and 55.7).  The DVF pass's field update, which
-// also writes the fields, was slower with it (97.0 to 103.9 ms).
+// 256x256x160: warp_fwd 47.4 to 37.3 ms per step, warp_back_add 59.6 to 55.2
+// ms with the fields and to 45.4 ms with the fields and the volume it updates
+// (1200 blocks ahead: 37.7 and 55.7; 300: 41.6 and 54.4).  The DVF pass's
+// field update, which also writes the fields, was slower with it (97.0 to
+// 103.9 ms).
 constexpr int WARP_PREFETCH_AHEAD = 600;
 
 // The prefetch for a block of a grid of 32 x TH tiles (gridDim.x x gridDim.y
@@ -226,7 +228,7 @@ static __global__ void __launch_bounds__(256) warp_back_add_kernel(
     const int tx = threadIdx.x, ty = threadIdx.y;
     const int xm = blockIdx.x * 32 + tx, iz = blockIdx.z;
     const int64_t slice = (int64_t)iz * nx * ny;
-    prefetch_tile_rows(f, nullptr, 8 * WR, nx, ny, nz, ty * 32 + tx);
+    prefetch_tile_rows(f, img, 8 * WR, nx, ny, nz, ty * 32 + tx);  // and the volume's rows
     if (xm >= nx) return;
 #pragma unroll
     for (int k = 0; k < WR; k++) {
