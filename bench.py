@@ -158,6 +158,8 @@ def algorithmic_bytes(p) -> dict:
         "fp_motion": 12 * V + 4 * P + 8 * P,
         # read the pairs; write the ratio volume
         "bp_div": 8 * P + 4 * V,
+        # the same in the DVF pass when it runs as its own launch
+        "bp_div_motion": 8 * P + 4 * V,
         # read volume (+ its update), write volume and its y-fastest copy
         "bp_div_add": 8 * P + 12 * V,
         # read img, 6 fields; write the warped volume in the layout the
@@ -174,6 +176,10 @@ def algorithmic_bytes(p) -> dict:
         # the two above in one pass: read ratio, img, read+write 6 fields,
         # write img0 and ones in the layout the next view's projector reads
         "field_update_prep": 8 * V + 48 * V + 8 * V,
+        # the DVF pass's backprojector and field update in one kernel: read
+        # the pairs, img, read+write 6 fields, write img0 and ones (the ratio
+        # stays on chip)
+        "bp_field_update_prep": 8 * P + 4 * V + 48 * V + 8 * V,
     }
 
 
@@ -183,13 +189,14 @@ def algorithmic_bytes(p) -> dict:
 # commands are kept under profiles/.
 NCU_DRAM_BYTES = {
     "motion256": {"fp_motion": 132078080, "fp_image": 42956032, "bp_div": 2872064,
-           "field_update_prep": 613819647},
+                  "field_update_prep": 613819647, "bp_field_update_prep": 573643208},
 }
 
 # Issue-slot utilisation (smsp__issue_active) of the projector and
 # backprojector from the same captures: these kernels are bound by issue and
 # latency, not by HBM.
-NCU_ISSUE_ACTIVE = {"motion256": {"fp_image": 0.570, "fp_motion": 0.602, "bp_div": 0.803}}
+NCU_ISSUE_ACTIVE = {"motion256": {"fp_image": 0.570, "fp_motion": 0.602, "bp_div": 0.817,
+                                  "bp_field_update_prep": 0.663}}
 
 # Views per pass of the CPU samples: the engine line's cpu_baseline leg
 # (about 10 s of CPU work) and each step of the reference arm (a few seconds,

@@ -293,7 +293,8 @@ int mcsart_batch_run(mcsart_ctx *ctx, const mcsart_problem *problems, int n_prob
  * src/cu_backprojection.cu:46, src/cu_deform.cu:5).  Times the candidate
  * shapes of the driver's per-view kernels (projector slab-group depth and
  * blocks per SM, backprojector voxels per thread and rows per block, warp
- * rows per thread, the DVF-pass field update's load order) on a sample of the problem's views (an image pass and a
+ * rows per thread, the DVF-pass field update: with the backprojection ratio computed inside it, or after a
+ * separate backprojector launch with either load order) on a sample of the problem's views (an image pass and a
  * DVF-update pass over up to 12 views, on copies of the image and fields;
  * the problem's buffers are not changed) and caches the fastest for the
  * problem's geometry and opt->storage.  Later driver runs of that geometry

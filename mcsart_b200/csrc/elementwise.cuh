@@ -4,6 +4,7 @@
 // the engine's driver uses instead of chains of them.
 #pragma once
 
+#include "backprojector.cuh"
 #include "common.cuh"
 #include "warp.cuh"
 
@@ -303,11 +304,21 @@ static __global__ void __launch_bounds__(256) field_update_kernel(FT *ax, FT *ay
 // that 24 loads per thread are in flight at once (more registers, fewer
 // resident blocks); otherwise the fields are loaded voxel by voxel.
 // PAIR: img0 and ones interleaved, as in motion_prep_kernel.
-template <typename FT, typename VT, bool EARLY = false, bool PAIR = false>
+// BP: the view's backprojection ratio of tile A (the DVF pass's
+// host_backprojection and host_division, src/AUMISART.cu:264-270) is
+// computed here from `bp` (its (residual, initial2-projection) pairs and
+// column data, one slice) with the backprojector's own per-voxel code,
+// instead of being read from img_temp: the field update of a tile needs the
+// ratio of that tile only, so the ratio never goes to memory, and blocks
+// gathering from the detector (bound by instruction issue) share the SMs
+// with blocks streaming the fields (bound by memory latency).  PROVEN: as in
+// bp_kernel.  The ratio's bits are the backprojector kernel's.
+template <typename FT, typename VT, bool EARLY = false, bool PAIR = false, bool BP = false,
+          bool PROVEN = false>
 static __global__ void __launch_bounds__(256) field_update_prep_kernel(
     FT *ax, FT *ay, FT *az, FT *bx, FT *by, FT *bz, const float *img_temp, const float *img,
     int nx, int ny, int nz, float nvd, float nfd, VT *img0, VT *img0T, VT *ones, VT *onesT,
-    float vd, float fd) {
+    float vd, float fd, const BPArgs bp) {
     __shared__ float ft[6][32][33];
     __shared__ float rt[32][33];
     __shared__ float o0[32][33], o1[32][33];
@@ -334,7 +345,19 @@ static __global__ void __launch_bounds__(256) field_update_prep_kernel(
 #pragma unroll
     for (int k = 0; k < 4; k++) {
         const int ly = ty + 8 * k, xx = x0 + tx, yy = y0 + ly;
-        rt[ly][tx] = (xx < nx && yy < ny) ? img_temp[xx + (int64_t)yy * nx + slice] : 0.0f;
+        float q = 0.0f;
+        if (xx < nx && yy < ny) {
+            if (BP) {
+                float a0 = 0.0f, a1 = 0.0f;
+                bp_gather_view<2, PROVEN, 1>(bp, bp.angle, nullptr, bp.pair, xx, yy, iz, &a0,
+                                             &a1);
+                q = a0 / a1;                           // cu_division.cu:20
+                if (isnan(q) || isinf(q)) q = 0.0f;    // :21-24
+            } else {
+                q = img_temp[xx + (int64_t)yy * nx + slice];
+            }
+        }
+        rt[ly][tx] = q;
     }
     __syncthreads();
     // field update on A^T: voxel (x', y') = (y0 + tx, x0 + lx); its q is the

@@ -222,7 +222,24 @@ template <typename ST, int INTERP, int SUM> struct Runner {
         return MCSART_OK;
     }
 
-    int launch_bp(int v, int mode, float *out, float *outT, cudaSurfaceObject_t surf = 0) {
+    // The backprojector's inputs for view v: the projector's (residual,
+    // ones-projection) pairs and, when that launch wrote them, its column data.
+    BPArgs bp_args(int v) {
+        BPArgs b{};
+        b.pair = S.pairs.as<float2>();
+        b.g = P.g;
+        b.angle = P.angles[v];
+        b.lambda = P.lambda;
+        if (cols_view == v) {
+            b.colA = S.bpcolA.as<float4>();
+            b.colB = S.bpcolB.as<float>();
+        }
+        return b;
+    }
+
+    // label: the profile label (default bp_div / bp_div_add by mode)
+    int launch_bp(int v, int mode, float *out, float *outT, cudaSurfaceObject_t surf = 0,
+                  const char *label = nullptr) {
         BPArgs b{};
         b.outSurf = surf;
         b.pair = S.pairs.as<float2>();
@@ -235,7 +252,7 @@ template <typename ST, int INTERP, int SUM> struct Runner {
             b.colA = S.bpcolA.as<float4>();
             b.colB = S.bpcolB.as<float>();
         }
-        ctx->label = mode == BP_DIV ? "bp_div" : "bp_div_add";
+        ctx->label = label ? label : mode == BP_DIV ? "bp_div" : "bp_div_add";
         if (opt.geom64) {  // FP64 geometry and normaliser (no precomputed columns)
             b.colA = nullptr;
             b.colB = nullptr;
@@ -576,28 +593,46 @@ template <typename ST, int INTERP, int SUM> struct Runner {
                           (const float *)P.img, f, g.nx, g.ny, g.nz, vd, fd);
             }
             MC_TRY((launch_fp<3, false, ST>(vol, v, k, FP_MOTION)));
-            MC_TRY(launch_bp(v, BP_DIV, S.ratio.as<float>(), nullptr));
+            // square slices, FP32 geometry: the backprojection ratio is
+            // computed inside the field update (field_update_prep_kernel's
+            // BP form) unless the tuning chose a separate field update
+            const bool fused_bp = fuse && k + 1 < nm && !opt.geom64 && tune.fup <= 0;
+            if (!fused_bp)
+                MC_TRY(launch_bp(v, BP_DIV, S.ratio.as<float>(), nullptr, 0, "bp_div_motion"));
             const float nvd = P.volumes[v - 1] - P.volumes[v];  // :272-277
             const float nfd = P.flows[v - 1] - P.flows[v];
             if (fuse && k + 1 < nm) {
                 const int vn = views_mot[k + 1];
                 const float vdn = P.volumes[vn] - P.volumes[vn - 1];
                 const float fdn = P.flows[vn] - P.flows[vn - 1];
-                ctx->label = "field_update_prep";
+                ctx->label = fused_bp ? "bp_field_update_prep" : "field_update_prep";
                 ST *const o_std = reads_std[vn] ? ones_std : nullptr;
                 ST *const o_tr = reads_tr[vn] ? ones_tr : nullptr;
-                if (tune.fup == 1)
+                const BPArgs b = bp_args(v);
+                if (fused_bp && bp_geom_proven(g))
+                    MC_LAUNCH(ctx, (field_update_prep_kernel<ST, ST, false, pair, true, true>),
+                              tile_grid(), dim3(32, 8), 0, fw, fw + V, fw + 2 * V, fw + 3 * V,
+                              fw + 4 * V, fw + 5 * V, (const float *)nullptr, (const float *)P.img,
+                              g.nx, g.ny, g.nz, nvd, nfd, std_or_null(vn, S.img0),
+                              tr_or_null(vn, S.img0T), o_std, o_tr, vdn, fdn, b);
+                else if (fused_bp)
+                    MC_LAUNCH(ctx, (field_update_prep_kernel<ST, ST, false, pair, true, false>),
+                              tile_grid(), dim3(32, 8), 0, fw, fw + V, fw + 2 * V, fw + 3 * V,
+                              fw + 4 * V, fw + 5 * V, (const float *)nullptr, (const float *)P.img,
+                              g.nx, g.ny, g.nz, nvd, nfd, std_or_null(vn, S.img0),
+                              tr_or_null(vn, S.img0T), o_std, o_tr, vdn, fdn, b);
+                else if (tune.fup == 1)
                     MC_LAUNCH(ctx, (field_update_prep_kernel<ST, ST, true, pair>), tile_grid(),
                               dim3(32, 8), 0, fw, fw + V, fw + 2 * V, fw + 3 * V, fw + 4 * V,
                               fw + 5 * V, (const float *)S.ratio.as<float>(), (const float *)P.img,
                               g.nx, g.ny, g.nz, nvd, nfd, std_or_null(vn, S.img0),
-                              tr_or_null(vn, S.img0T), o_std, o_tr, vdn, fdn);
+                              tr_or_null(vn, S.img0T), o_std, o_tr, vdn, fdn, b);
                 else
                     MC_LAUNCH(ctx, (field_update_prep_kernel<ST, ST, false, pair>), tile_grid(),
                               dim3(32, 8), 0, fw, fw + V, fw + 2 * V, fw + 3 * V, fw + 4 * V,
                               fw + 5 * V, (const float *)S.ratio.as<float>(), (const float *)P.img,
                               g.nx, g.ny, g.nz, nvd, nfd, std_or_null(vn, S.img0),
-                              tr_or_null(vn, S.img0T), o_std, o_tr, vdn, fdn);
+                              tr_or_null(vn, S.img0T), o_std, o_tr, vdn, fdn, b);
             } else {
                 ctx->label = "field_update";
                 MC_LAUNCH(ctx, (field_update_kernel<ST>), tile_grid(), dim3(32, 8), 0, fw, fw + V,

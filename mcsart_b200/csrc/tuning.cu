@@ -34,8 +34,11 @@ namespace mcsart {
 //   bp   backprojector          0: 2 voxels/thread, 4 rows      1: 1 voxel, 4 rows
 //                               2: 2 voxels, 8 rows             3: 4 voxels, 4 rows
 //   warp image-pass warps       0: 2 rows/thread  1: 1 row  2: 4 rows
-//   fup  DVF-pass field update  0: fields loaded voxel by voxel  1: all loaded first
-constexpr int N_FP1 = 5, N_FP3 = 4, N_BP = 4, N_WARP = 3, N_FUP = 2;
+//   fup  DVF-pass field update  0: with the backprojection ratio computed in it
+//                               (square slices, FP32 geometry; else as 2)
+//                               1: after a backprojector launch, fields loaded first
+//                               2: after a backprojector launch, voxel by voxel
+constexpr int N_FP1 = 5, N_FP3 = 4, N_BP = 4, N_WARP = 3, N_FUP = 3;
 
 std::string tuning_key(const Geom &g, int storage) {
     char b[256];
@@ -64,6 +67,24 @@ double per_launch(const mcsart_ctx *ctx, std::initializer_list<const char *> lab
                 ms += e.second.ms;
                 n += e.second.launches;
             }
+    return n > 0 ? ms / (double)n : -1.0;
+}
+
+// Milliseconds per view of the DVF pass's backprojection and field update,
+// whether fused or as two launches: the time of both labels' launches over
+// the number of field-update launches (the pass's last view, a separate
+// backprojector and field update in every variant, counts in the sum).
+double per_view_field_update(const mcsart_ctx *ctx) {
+    double ms = 0.0;
+    long long n = 0;
+    for (const auto &e : ctx->prof_table) {
+        if (e.first == "bp_field_update_prep" || e.first == "field_update_prep") {
+            ms += e.second.ms;
+            n += e.second.launches;
+        } else if (e.first == "bp_div_motion") {
+            ms += e.second.ms;
+        }
+    }
     return n > 0 ? ms / (double)n : -1.0;
 }
 
@@ -126,7 +147,7 @@ int autotune_problem(mcsart_ctx *ctx, const Problem &P, const mcsart_options &op
             const double f3 = per_launch(ctx, {"fp_motion"});
             const double b = per_launch(ctx, {"bp_div", "bp_div_add"});
             const double w = per_launch(ctx, {"warp_fwd", "warp_back_add"});
-            const double u = per_launch(ctx, {"field_update_prep"});
+            const double u = per_view_field_update(ctx);
             if (f1 >= 0) best_fp1[trial.fp1] = std::min(best_fp1[trial.fp1], f1);
             if (f3 >= 0) best_fp3[trial.fp3] = std::min(best_fp3[trial.fp3], f3);
             if (b >= 0) best_bp[trial.bp] = std::min(best_bp[trial.bp], b);
@@ -181,7 +202,7 @@ MC_EXPORT int mcsart_tuning_save(mcsart_ctx *ctx, const char *path) {
     MC_REQUIRE(path, "path is NULL");
     FILE *f = fopen(path, "w");
     MC_REQUIRE(f, "cannot open %s for writing", path);
-    fprintf(f, "# mcsart tuning cache v2: key fp1 fp3 bp warp fup\n");
+    fprintf(f, "# mcsart tuning cache v3: key fp1 fp3 bp warp fup\n");
     for (const auto &e : ctx->tuning)
         fprintf(f, "%s %d %d %d %d %d\n", e.first.c_str(), e.second.fp1, e.second.fp3,
                 e.second.bp, e.second.warp, e.second.fup);

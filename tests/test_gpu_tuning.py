@@ -13,7 +13,7 @@ from test_gpu_sart import make_case
 
 pytestmark = pytest.mark.gpu
 
-N_VARIANTS = (5, 4, 4, 3, 2)  # fp1, fp3, bp, warp, fup
+N_VARIANTS = (5, 4, 4, 3, 3)  # fp1, fp3, bp, warp, fup
 
 
 def _run(ctx, torch, case, opt):
