@@ -189,7 +189,7 @@ def algorithmic_bytes(p) -> dict:
 # commands are kept under profiles/.
 NCU_DRAM_BYTES = {
     "motion256": {"fp_motion": 132078080, "fp_image": 42956032, "bp_div": 2872064,
-                  "field_update_prep": 613819647, "bp_field_update_prep": 573643208},
+                  "field_update_prep": 613819647, "bp_field_update_prep": 573643608},
 }
 
 # Issue-slot utilisation (smsp__issue_active) of the projector and
