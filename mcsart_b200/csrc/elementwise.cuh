@@ -325,6 +325,32 @@ static __global__ void __launch_bounds__(256) field_update_prep_kernel(
     const int tx = threadIdx.x, ty = threadIdx.y;
     const int x0 = blockIdx.x * 32, y0 = blockIdx.y * 32, iz = blockIdx.z;
     const int64_t slice = (int64_t)iz * nx * ny;
+    if (BP) {
+        // The block's own field rows (tile A^T) and volume rows (A^T and A)
+        // are prefetched into L2 before the backprojection gather, which
+        // then covers their memory latency: one 32-voxel row per thread
+        // (6 x 32 field rows, 2 x 32 volume rows).  Measured at 256x256x160:
+        // 151.4 to 141.9 ms per step (fields alone 145.3).
+        const int t = ty * 32 + tx, r = t % 32, w = t / 32;
+        const void *p = nullptr;
+        if (w < 7) {  // rows of A^T: memory rows x0 + r, columns from y0
+            if (x0 + r < ny && y0 < nx) {
+                const int64_t i = y0 + (int64_t)(x0 + r) * nx + slice;
+                switch (w) {
+                    case 0: p = ax + i; break;
+                    case 1: p = ay + i; break;
+                    case 2: p = az + i; break;
+                    case 3: p = bx + i; break;
+                    case 4: p = by + i; break;
+                    case 5: p = bz + i; break;
+                    default: p = img + i;
+                }
+            }
+        } else if (y0 + r < ny && x0 < nx) {  // volume rows of A
+            p = img + x0 + (int64_t)(y0 + r) * nx + slice;
+        }
+        if (p) asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+    }
     // the field values at this thread's 4 voxels of A^T (EARLY)
     float fe[EARLY ? 4 : 1][6];
     if (EARLY) {
