@@ -305,7 +305,7 @@ static __global__ void __launch_bounds__(256) field_update_kernel(FT *ax, FT *ay
 // resident blocks); otherwise the fields are loaded voxel by voxel.
 // PAIR: img0 and ones interleaved, as in motion_prep_kernel.
 // BP: the view's backprojection ratio of tile A (the DVF pass's
-// host_backprojection and host_division, src/AUMISART.cu:264-270) is
+// host_backprojection and host_division, src/AUMISART.cu:95-100 / :265-270) is
 // computed here from `bp` (its (residual, initial2-projection) pairs and
 // column data, one slice) with the backprojector's own per-voxel code,
 // instead of being read from img_temp: the field update of a tile needs the
