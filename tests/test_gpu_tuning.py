@@ -114,3 +114,49 @@ def test_malformed_tuning_file_is_rejected(ctx, tmp_path):
     p.write_text("somekey 9 0 0 0 0\n")
     with pytest.raises(m.McsartError):
         ctx.tuning_load(p)
+
+
+@pytest.mark.parametrize("storage", [1, 2])
+def test_fused_and_separate_dvf_field_updates_agree_with_16bit_storage(ctx, torch_cuda, oracle,
+                                                                       tmp_path, storage):
+    """The DVF pass's field update with the backprojection computed inside it
+    (variant 0, the built-in choice) and after a separate backprojector launch
+    (variants 1 and 2) give the same bits with BF16 and FP16 fields and
+    projections too (the ratio is computed from the FP32 pairs either way)."""
+    import mcsart_b200 as m
+    torch = torch_cuda
+    dt = torch.bfloat16 if storage == m.BF16 else torch.float16
+    g, it, img0, proj, F = make_case(oracle, motion=True, op_iter=(1, 0, 1), seed=24, nx=32,
+                                     ny=32, nz=20, na=48, nb=40)
+    opt = m.default_options(storage=storage)
+
+    def run(c):
+        d_img = dev(torch, img0)
+        d_F = dev(torch, np.stack(F)).to(dt)
+        c.aumisart_device(geo=g, n_views=it["n_views"], lambda_=1.0, angles=it["angles"],
+                          volumes=it["volumes"], flows=it["flows"], img=d_img,
+                          proj=dev(torch, proj).to(dt), fields=d_F, n_iter=it["n_iter"],
+                          op_iter=it["op_iter"], options=opt)
+        c.synchronize()
+        return host(d_img), host(d_F.float())
+
+    with m.Context(0, stream=torch.cuda.current_stream().cuda_stream) as c:
+        c.autotune(geo=g, n_views=it["n_views"], lambda_=1.0, angles=it["angles"],
+                   volumes=it["volumes"], flows=it["flows"], img=dev(torch, img0),
+                   proj=dev(torch, proj).to(dt), fields=dev(torch, np.stack(F)).to(dt),
+                   options=opt)
+        path = tmp_path / "t.txt"
+        c.tuning_save(path)
+        key = [ln.split()[0] for ln in open(path).read().splitlines()
+               if not ln.startswith("#") and ln.split()[0].endswith(f"/s{storage}")][0]
+    results = []
+    for fup in (0, 1, 2):
+        p = tmp_path / f"forced{fup}.txt"
+        p.write_text(f"{key} -1 -1 -1 -1 {fup}\n")
+        with m.Context(0, stream=torch.cuda.current_stream().cuda_stream) as c:
+            assert c.tuning_load(p) == 1
+            assert c.tuning_get(g, storage)[4] == fup
+            results.append(run(c))
+    for r in results[1:]:
+        np.testing.assert_array_equal(r[0], results[0][0])
+        np.testing.assert_array_equal(r[1], results[0][1])
